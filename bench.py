@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the integrating-factor RK3 pseudo-spectral step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the forced inverse-cascade configuration at 1024^2, FP32 FFT): one
+benchmark step is one substep of the reference's frame loop, i.e. one RK3 step
+(3 stages, 9 FFTs) + BFECC dye advection on the 2x refined 2048^2 dye grid +
+the CFL reduction; white-in-time stochastic forcing in the annulus |k| = 64+-2
+(amplitude 0.1), order-4 hyperviscosity nu4 = 1e-16, drag 1e-2, beta 0,
+CFL 0.5 capped at dt = 1e-3; seeded band-limited initial field (4 <= |k| <= 12,
+rms vorticity 1).  Inputs are synthetic and generated on the device.
+
+Rank 0 prints ONE JSON line.  ``value`` is device-timed whole-job steps/s
+(CUDA events on the solver stream, barrier + synchronize around the timed
+region, max over ranks; N ranks run N independent replicas: "replicas only",
+weak scaling).  ``e2e`` is the same metric through the public Solver API with
+per-step host->device parameter/splat uploads and a device->host diagnostics
+read inside the timed region.  ``roofline`` covers the dominant kernel,
+``cpu_baseline`` the FP64 NumPy restatement of reference/spectral2d.py on the
+host, ``ensemble`` the batched 256 x 256^2 ensemble.
+
+``--impl reference`` times the reference's CPU algorithm (the oracle port of
+reference/spectral2d.py, NumPy FP64) on the same workload with every host core
+running one replica, and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "RK3 steps/s (1024^2; 256x256^2 batch): TC split-FFT vs FP32 at rel err <=1e-5"
+UNIT = "steps/s"
+N = 1024
+DYE_SCALE = 2
+NU4 = 1e-16
+HYPER_P = 4
+CFG = {"beta": 0.0, "drag": 1e-2, "viscosity": NU4 * (N / 3.0) ** (2 * HYPER_P), "hyperP": HYPER_P,
+       "forceAmp": 0.1, "forceK": 64.0, "forceWidth": 2.0, "cfl": 0.5, "dtMin": 1e-6, "dtMax": 1e-3,
+       "dyeFade": 0.999}
+WORKLOAD = "forced inverse cascade 1024^2 FP32, dye 2048^2 (config 2 of the reference benchmark set)"
+L2_BYTES = 126 * 2 ** 20
+
+
+def _rows_in_band(n):
+    kcut = n / 3.0
+    return sum(1 for i in range(n) if abs(i if i < n // 2 else i - n) < kcut)
+
+
+def algorithmic_bytes(n, m):
+    """Per-launch algorithmic HBM bytes of each kernel class (averaged over the 3 stages)."""
+    rb = _rows_in_band(n)
+    c = 8 * n * n
+    phys = 2 * c + 8 * n * rb + c / 3.0                  # PA+PB read, in-band Z rows written, vel at stage 2
+    spec = 8 * n * rb + 4 * c + 2 * c / 3.0              # Z rows, wcur, wout, PA, PB; w0 at stages 1-2
+    dye = 56 * m * m + 24 * n * n                        # 3 passes over rgba16f textures + velocity reads
+    return {"phys_cols": phys, "spec_rows": spec, "dye": dye}
+
+
+def step_algorithmic_bytes(n):
+    """Minimum-pass dataflow of one RK3 step, 232 N^2 bytes (dye and pointer forcing excluded)."""
+    return 232 * n * n
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def committed_traffic(kernel):
+    """DRAM bytes per launch of `kernel` recorded from an ncu capture under profiles/."""
+    pat = re.compile(r"^traffic_bytes_per_launch\s+(\S+)\s+([0-9.eE+]+)")
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(d, f)) as fh:
+            for line in fh:
+                m = pat.match(line.strip())
+                if m and m.group(1) == kernel:
+                    return float(m.group(2))
+    return None
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ CPU reference arm
+def _oracle_worker(args):
+    """Run `steps` oracle RK3 steps on the workload; returns (steps, seconds)."""
+    n, steps, seed = args
+    import numpy as np
+    from oracle import wgsl_oracle as wo
+    from oracle.spectral_oracle import SpectralOracle, band_noise_spectrum
+    nu_h = float(wo.nu_h_from_rate(CFG["viscosity"], n, HYPER_P))
+    s = SpectralOracle(n=n, beta=CFG["beta"], mu=CFG["drag"], nu_h=nu_h, hyper_p=HYPER_P, cfl=CFG["cfl"],
+                       dt_max=CFG["dtMax"])
+    s.w = band_noise_spectrum(n, 4, 12, seed)
+    s.step(dt=CFG["dtMax"])        # warm-up
+    t0 = time.perf_counter()
+    for k in range(steps):
+        dt = s.timestep()
+        f = wo.stochastic_forcing(n, CFG["forceAmp"], CFG["forceK"], CFG["forceWidth"], k, dt)
+        s.step(dt=dt, forcing=f.astype(np.complex128))
+    return steps, time.perf_counter() - t0
+
+
+def cpu_baseline(budget_s=15.0):
+    """The FP64 NumPy restatement of reference/spectral2d.py, one core, bounded sample."""
+    steps1, t1 = _oracle_worker((N, 1, 0))
+    k = max(1, min(20, int(budget_s / max(t1, 1e-3))))
+    steps, secs = _oracle_worker((N, k, 0))
+    return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} RK3 steps of one {N}^2 instance with forcing and CFL dt "
+                      f"(FP64 NumPy restatement of reference/spectral2d.py, no dye), {secs:.1f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    # bound the run: each replica does at most what fits ~90 s of host time
+    _, t1 = _oracle_worker((N, 1, 0))
+    per = max(1, min(args.steps, int(90.0 / max(t1, 1e-3))))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, [(N, per, r) for r in range(procs)])
+    wall = time.perf_counter() - t0
+    steps = sum(r[0] for r in res)
+    secs = max(r[1] for r in res)
+    value = steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / per,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": N, "replicas": procs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{procs} processes x {per} RK3 steps at {N}^2 (NumPy FP64 restatement of "
+                                   f"reference/spectral2d.py; wall {wall:.1f} s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    dev = local
+    torch.cuda.set_device(dev)
+
+    solver = pkg.Solver.create(device=dev, n=N, dyeScale=DYE_SCALE)
+    solver.configure(CFG)
+    solver.reset({"k0": 14, "amplitude": 0, "seed": 1, "dyePattern": "bands"})
+    solver.seedBand(4.0, 12.0, rms=1.0, seed=1 + rank)
+    stream = torch.cuda.ExternalStream(solver.stream, device=dev)
+
+    # warm-up (also captures the graphs of the 6 (phase, dt slot, dye parity) combinations)
+    solver.step(max(args.warmup, 6), dye=True, reduce=True, graph=True, relatch=True)
+    solver.synchronize()
+
+    # ---- device-timed region
+    clocks = ClockSampler(dev)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    solver.step(args.steps, dye=True, reduce=True, graph=True, relatch=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world)
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- RK3-only (no dye) for reference
+    solver.step(3, dye=False, reduce=True, graph=True, relatch=True)
+    solver.synchronize()
+    ev0.record(stream)
+    solver.step(args.steps, dye=False, reduce=True, graph=True, relatch=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms_rk3 = max_over_ranks(ev0.elapsed_time(ev1), world)
+
+    # ---- per-kernel device times (event pairs around each launch, non-graph path)
+    ksteps = min(args.steps, 60)
+    solver.profile(True)
+    solver.step(ksteps, dye=True, reduce=True, graph=False, relatch=True)
+    prof = solver.profileRead()
+    solver.profile(False)
+    ab = algorithmic_bytes(N, N * DYE_SCALE)
+    hbm, bf16, peak_src = load_peaks()
+    dom = max(("phys_cols", "spec_rows", "dye"), key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    avg_launch_s = dom_ms / 1e3 / max(dom_n, 1)
+    achieved = ab[dom] / avg_launch_s / 1e9
+    kernel_names = {"phys_cols": "k_phys_cols", "spec_rows": "k_spec_rows", "dye": "k_dye (3 passes)"}
+    traffic = committed_traffic(kernel_names[dom].split()[0])
+    step_ms = ms / args.steps if world == 1 else ms / args.steps
+    roofline = {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": ab[dom], "avg_launch_ms": avg_launch_s * 1e3,
+                "per_kernel_ms_per_step": {k: prof[k][0] / ksteps for k in prof}}
+    step_roof = step_algorithmic_bytes(N) / ((ms_rk3 / args.steps) / 1e3) / 1e9
+
+    # ---- end to end through the public API: per step configure + splats + step + diagnostics read
+    e2e_steps = min(args.steps, 200)
+    for _ in range(3):
+        solver.configure(CFG)
+        solver.setSplats([])
+        solver.step(1, dye=True, reduce=True, graph=True)
+        solver.encodeDiagnostics()
+        solver.copyDiagnostics()
+        solver.readDiagnostics()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.configure(CFG)                       # H2D: parameter block (re-latches stepIndex)
+        solver.setSplats([])                        # H2D: splat block
+        solver.step(1, dye=True, reduce=True, graph=True)
+        solver.encodeDiagnostics()
+        solver.copyDiagnostics()
+        d = solver.readDiagnostics()                # D2H: spectrum, zonal, dt, energy, enstrophy
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * e2e_steps / e2e_s
+    nb = N // 2 + 1
+    h2d = 64 + 16 + 8 * 48
+    d2h = (nb + 2) * 8 + (nb + 2) * 4 + N * 4 + 2 * 4
+    finite = d is not None and all(map(lambda v: v == v, [d["energy"], d["enstrophy"], d["dt"]]))
+    solver.destroy()
+
+    # ---- batched ensemble: 256 instances of 256^2 (sharded across ranks)
+    ens = None
+    if not args.no_ensemble:
+        ens = run_ensemble(pkg, torch, world, rank, dev, args)
+
+    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu) else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N, "dye": N * DYE_SCALE, "fft": "fp32 CUDA-core",
+                       "parallelism": f"replicas x{world}", "graph": True,
+                       "l2": f"no flush; per-step working set {working_set(N, N * DYE_SCALE) / 2**20:.0f} MiB "
+                             f"> L2 {L2_BYTES / 2**20:.0f} MiB",
+                       "forcing": "white-in-time, |k|=64+-2, amp 0.1", "dt": "CFL 0.5, max 1e-3"},
+            "rk3_only_steps_per_s": world * args.steps / (ms_rk3 / 1e3),
+            "step_roofline": {"bytes_per_step": step_algorithmic_bytes(N), "achieved_gbs": step_roof,
+                              "frac": step_roof / hbm, "note": "232 N^2 algorithmic bytes per RK3 step (no dye)"},
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps, "diagnostics_finite": bool(finite)},
+            "gpu_launches": args.steps * 10,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "ensemble": ens,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def working_set(n, m):
+    return 8 * n * n * 7 + 8 * m * m * 3
+
+
+def run_ensemble(pkg, torch, world, rank, dev, args):
+    import numpy as np
+    rng = np.random.default_rng(1234)
+    count_total = 256
+    inst = []
+    for i in range(count_total):
+        inst.append({"n": 256, "beta": float(rng.uniform(0, 20)), "drag": float(rng.uniform(0, 2e-2)),
+                     "nuH": float(rng.uniform(1e-4, 1e-3)), "hyperP": 1, "dt": 2e-3, "seed": i})
+    mine = inst[rank::world]
+    e = pkg.Ensemble(mine, device=dev)
+    e.seedBand(4.0, 12.0, rms=1.0)
+    stream = torch.cuda.ExternalStream(e.stream, device=dev)
+    e.step(6, graph=True)
+    e.synchronize()
+    steps = max(3, (min(args.steps, 300) // 3) * 3)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e.step(steps, graph=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier(world)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    en, _ = e.energy()
+    ok = bool(np.all(np.isfinite(en)))
+    e.destroy()
+    hbm, _, _ = load_peaks()
+    ens_steps_per_s = steps / (ms / 1e3)
+    bytes_step = step_algorithmic_bytes(256) * count_total
+    gbs = bytes_step * ens_steps_per_s / 1e9
+    return {"instances": count_total, "n": 256, "ensemble_steps_per_s": ens_steps_per_s,
+            "instance_steps_per_s": ens_steps_per_s * count_total, "ms_per_ensemble_step": ms / steps,
+            "achieved_gbs": gbs, "hbm_peak_gbs": hbm, "frac_of_hbm": gbs / hbm, "finite": ok,
+            "note": "232 N^2 algorithmic bytes per instance-step; per-instance nu, beta, drag; graph-replayed"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,249 @@
+/*
+ * s2d.h -- C ABI of the B200 pseudo-spectral vorticity solver.
+ *
+ * This is the drop-in boundary for the reference's JavaScript solver API
+ * (src/gpu/solver.js `class Solver`, src/gpu/fft.js `Fft2D`/`radixSchedule`,
+ * src/gpu/device.js `supportedGrids`).  Each entry point names the reference
+ * interface it replaces (file:line).  Plain C types only: pointers, sizes,
+ * ints and floats.  Every call returns an int status (S2D_OK = 0, errors < 0);
+ * the N-API / ctypes shims turn a negative status into a thrown Error with the
+ * text of s2d_last_error().
+ *
+ * Data layout (identical to the reference buffers): a spectral field is N*N
+ * interleaved complex64 (re, im float pairs), row-major, row = y index with
+ * ky = wn(row), column = x index with kx = wn(col), wn(i) = i < N/2 ? i : i-N.
+ * The dye is M*M texels of 4 binary16 values (rgba16float), M = N*dye_scale.
+ *
+ * Threading: a solver handle is used from one host thread at a time; all GPU
+ * work of one solver is ordered on the solver's own CUDA stream.
+ */
+#ifndef S2D_H
+#define S2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define S2D_OK 0
+#define S2D_NO_DATA 1             /* readDiagnostics resolved to null (solver.js:571-573) */
+#define S2D_ERR_ARG (-1)          /* bad argument / null handle                              */
+#define S2D_ERR_UNSUPPORTED_N (-2)/* grid size not supported (fft.js:27-29)                 */
+#define S2D_ERR_CUDA (-3)         /* CUDA runtime error (text in s2d_last_error)             */
+#define S2D_ERR_DESTROYED (-4)    /* use after destroy (solver.js:571, 614-615)              */
+#define S2D_ERR_NAN (-5)          /* non-finite value found in a host-provided field         */
+#define S2D_ERR_UNREGISTERED (-6) /* FFT on a buffer never registered (fft.js:84)            */
+#define S2D_ERR_NO_DEVICE (-7)    /* no CUDA device / wrong architecture                     */
+
+/* ---------------------------------------------------------------- limits */
+#define S2D_MAX_SPLATS 8          /* MAX_SPLATS, solver.js:9 */
+#define S2D_MIN_N 32
+#define S2D_MAX_N 4096
+
+/* buffer ids of the per-stage test hooks (tests/index.html:120-201 names) */
+enum s2d_buffer_id {
+  S2D_BUF_STATE0 = 0, S2D_BUF_STATE1 = 1, S2D_BUF_STATE2 = 2,
+  S2D_BUF_PACKA = 3, S2D_BUF_PACKB = 4, S2D_BUF_PHYSZ = 5,
+  S2D_BUF_RHS = 6, S2D_BUF_FORCE = 7,
+  S2D_BUF_VEL = 8,      /* N*N float2 (u, v), physical space */
+  S2D_BUF_DT = 9        /* 4 floats: [dt, maxSpeed, 0, 0] of the current dt slot */
+};
+
+/* step flags: one substep of the main.js:413-419 loop is
+ * encodeStep, then encodeDye, then encodeReduce */
+#define S2D_STEP_DYE 1u
+#define S2D_STEP_REDUCE 2u
+/* Re-latch the stochastic-forcing step index before every substep, as a
+ * configure() call before each substep would (main.js:403 calls configure once
+ * per frame, so with one substep per frame every step gets a fresh phase). */
+#define S2D_STEP_RELATCH 4u
+
+/* FFT arithmetic of the fused step */
+#define S2D_FFT_FP32 0            /* CUDA-core FP32 FFT */
+#define S2D_FFT_TC_F16 1          /* tensor-core DFT-GEMM, FP16 hi+lo split, FP32 accumulate */
+#define S2D_FFT_TC_BF16 2         /* tensor-core DFT-GEMM, BF16 hi+mid+lo split, FP32 accumulate */
+
+/* dye patterns of paintDye (solver.js:446-473) */
+#define S2D_DYE_NONE 0
+#define S2D_DYE_BANDS 1
+
+/* Solver.configure(cfg) keys (solver.js:306-324).  `viscosity` is the damping
+ * RATE at the dealias cutoff; nuH = viscosity / (N/3)^(2*hyperP) (solver.js:311). */
+typedef struct s2d_params {
+  float beta, drag, viscosity;
+  int32_t hyper_p;
+  float force_amp, force_k, force_width;
+  float cfl, dt_min, dt_max;
+  float dye_fade;
+} s2d_params;
+
+/* setSplats list entry (solver.js:326-345; built by ui/pointer.js:57-67).
+ * x, y in [0,1)^2; (dx, dy) the stroke velocity; colour in [0,1]. */
+typedef struct s2d_splat {
+  float x, y, dx, dy;
+  float color[3];
+  float radius, amp, dye_amp;
+} s2d_splat;
+
+/* scalar state fields of the JS Solver (solver.js:50-69) */
+typedef struct s2d_info {
+  int32_t n, m, nbins;
+  int32_t phase, dye_parity;
+  uint32_t step_index;
+  int32_t primed;
+  int32_t fft_precision;
+  float nu_h;           /* paramsF[2] */
+  double sim_time;
+} s2d_info;
+
+typedef struct s2d_solver s2d_solver;
+
+/* ---------------------------------------------------------------- library */
+int s2d_version(void);
+const char* s2d_status_string(int status);
+const char* s2d_last_error(void);
+
+/* radixSchedule(n) (fft.js:20-31): stages of radix 4 and whether a radix-2 tail
+ * is present; S2D_ERR_UNSUPPORTED_N for n not of the form 4^a or 2*4^a. */
+int s2d_radix_schedule(int n, int* stages, int* has_radix2);
+/* supportedGrids(limits) (device.js:44-52), re-derived for the current B200:
+ * writes the supported sizes in [S2D_MIN_N, S2D_MAX_N] ascending. */
+int s2d_supported_grids(int* out, int capacity, int* count);
+/* Bit-exact tables computed by GPU kernels (for parity tests):
+ * digit reversal over the reversed radix list (fft.wgsl:32-40, fft_ref.py:19-24),
+ * wn(i) as float (common.wgsl:50-55), and the 2/3 dealias mask (common.wgsl:69-74). */
+int s2d_digit_reverse_table(int n, uint32_t* out /* n */);
+int s2d_wavenumber_table(int n, float* out /* n */);
+int s2d_dealias_mask_table(int n, uint8_t* out /* n*n */);
+
+/* ---------------------------------------------------------------- lifecycle */
+/* Solver.create(device, {n, dyeScale}) (solver.js:71-140). */
+int s2d_create(int n, int dye_scale, int fft_precision, int device, s2d_solver** out);
+/* Solver.destroy() (solver.js:614-629); the handle is freed. */
+int s2d_destroy(s2d_solver* s);
+int s2d_get_info(s2d_solver* s, s2d_info* out);
+/* solver.phase / dyeParity / simTime assignments made by tests/index.html:162,185-186 */
+int s2d_set_phase(s2d_solver* s, int phase, int dye_parity);
+int s2d_set_sim_time(s2d_solver* s, double t);
+/* CUDA stream the solver enqueues on (cudaStream_t as void*). */
+int s2d_get_stream(s2d_solver* s, void** stream);
+int s2d_synchronize(s2d_solver* s);
+
+/* ---------------------------------------------------------------- parameters */
+int s2d_configure(s2d_solver* s, const s2d_params* p);                   /* solver.js:306-324 */
+int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count);     /* solver.js:326-345 */
+
+/* ---------------------------------------------------------------- seeding */
+/* seed({k0, amplitude, seed}) (solver.js:347-359, fillSpectrum 384-418). */
+int s2d_seed(s2d_solver* s, double k0, double amplitude, uint32_t seed);
+/* seedPhysical(Float32Array N*N) (solver.js:361-382): FFT + dealias mask into state 0. */
+int s2d_seed_physical(s2d_solver* s, const float* field);
+/* reset({field} | {k0, amplitude, seed, dyePattern}) (solver.js:420-444);
+ * field == NULL selects spectral seeding. */
+int s2d_reset(s2d_solver* s, const float* field, double k0, double amplitude, uint32_t seed,
+              int dye_pattern);
+int s2d_paint_dye(s2d_solver* s, int pattern);                           /* solver.js:446-473 */
+/* Band-limited initial spectrum of the benchmark workloads: complex Gaussian
+ * noise (counter-based, from `seed`) kept in kmin <= |k| <= kmax,
+ * Hermitian-symmetrised, dealias-masked, k=0 removed, scaled to rms vorticity
+ * `rms`; into state 0 with the other states cleared.  No reference
+ * counterpart (the reference seeds with fillSpectrum or a physical field). */
+int s2d_seed_band(s2d_solver* s, float kmin, float kmax, float rms, uint32_t seed);
+
+/* ---------------------------------------------------------------- step */
+int s2d_encode_prime(s2d_solver* s);                                     /* solver.js:475-486 */
+int s2d_encode_step(s2d_solver* s);                                      /* solver.js:488-521 */
+int s2d_encode_dye(s2d_solver* s);                                       /* solver.js:523-536 */
+int s2d_encode_reduce(s2d_solver* s);                                    /* solver.js:538-545 */
+/* `substeps` repetitions of encodeStep (+ encodeDye, + encodeReduce per flags),
+ * priming first when needed: the body of main.js:409-419. */
+int s2d_step(s2d_solver* s, int substeps, unsigned flags);
+/* As s2d_step, replayed from a captured CUDA graph of one substep. */
+int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags);
+
+/* ---------------------------------------------------------------- diagnostics */
+int s2d_encode_diagnostics(s2d_solver* s);                               /* solver.js:547-558 */
+int s2d_copy_diagnostics(s2d_solver* s);                                 /* solver.js:560-568 */
+/* 1 when the copied diagnostics have landed in host memory, 0 otherwise. */
+int s2d_poll_diagnostics(s2d_solver* s);
+/* readDiagnostics() (solver.js:570-608): waits for the copy; S2D_NO_DATA when
+ * nothing was copied (the JS null).  Spectrum, energy and enstrophy are FP64
+ * reductions of the current state; zonal is the mean over x of u of the
+ * velocity of the last RK stage-2 evaluation (the reference's packA.y). */
+int s2d_read_diagnostics(s2d_solver* s, double* spectrum /* N/2+1 */, float* zonal /* N */,
+                         double* energy, double* enstrophy, float* dt, float* max_speed);
+/* The reference's fixed-point decoding of the same quantities
+ * (spectrum.wgsl:19-39 accumulation, solver.js:591-602 decoding). */
+int s2d_read_diagnostics_fixed(s2d_solver* s, float* spectrum /* N/2+1 */, float* energy,
+                               float* enstrophy);
+
+/* ---------------------------------------------------------------- stage hooks */
+int s2d_get_buffer(s2d_solver* s, int id, void* host, size_t bytes);
+int s2d_set_buffer(s2d_solver* s, int id, const void* host, size_t bytes);
+/* Fft2D.forward/inverse(pass, name) (fft.js:81-101) on packA/packB/physZ/force;
+ * other ids give S2D_ERR_UNREGISTERED.  Inverse scales 1/N per axis. */
+int s2d_fft2(s2d_solver* s, int id, int inverse);
+/* velocity_pack from state[state_index] into packA/packB (solver.wgsl:21-40). */
+int s2d_velocity_pack(s2d_solver* s, int state_index);
+/* nl_pack: packA/packB -> physZ, vel (solver.wgsl:42-54). */
+int s2d_nl_pack(s2d_solver* s);
+/* assemble: physZ, force, dt -> rhs (solver.wgsl:56-95). */
+int s2d_assemble(s2d_solver* s);
+/* rk3 stage update with the current phase's state ring (solver.wgsl:103-122). */
+int s2d_rk3_stage(s2d_solver* s, int stage);
+/* currentDye (solver.js:610-612): copies M*M*4 binary16 values. */
+int s2d_get_dye(s2d_solver* s, uint16_t* out);
+int s2d_set_dye(s2d_solver* s, const uint16_t* in);
+
+/* ---------------------------------------------------------------- instrumentation */
+/* Kernel classes timed by the profiler: the two fused stage kernels, the dye
+ * passes, the pointer force (field + FFT) and everything else. */
+#define S2D_PROF_PHYS_COLS 0
+#define S2D_PROF_SPEC_ROWS 1
+#define S2D_PROF_DYE 2
+#define S2D_PROF_FORCE 3
+#define S2D_PROF_OTHER 4
+#define S2D_PROF_CLASSES 5
+/* enable != 0 starts recording a CUDA event pair around every kernel the
+ * non-graph entry points launch (no reference counterpart); 0 stops. */
+int s2d_profile(s2d_solver* s, int enable);
+/* Synchronizes, then returns the summed device time (ms) and launch count per
+ * class since the last read, and clears them. */
+int s2d_profile_read(s2d_solver* s, double* ms /* S2D_PROF_CLASSES */, int* launches /* S2D_PROF_CLASSES */);
+
+/* ---------------------------------------------------------------- ensemble */
+/* Many independent instances of uneven sizes stepped together (no reference
+ * counterpart beyond running many Solvers; BASELINE batching form). */
+typedef struct s2d_instance_desc {
+  int32_t n;              /* 32..512, power of two */
+  float beta, drag, nu_h; /* nu_h directly (not the rate) */
+  int32_t hyper_p;
+  float dt;               /* fixed step of this instance */
+  float force_amp, force_k, force_width;
+  uint32_t seed;
+} s2d_instance_desc;
+
+typedef struct s2d_ensemble s2d_ensemble;
+
+int s2d_ensemble_create(const s2d_instance_desc* descs, int count, int device,
+                        s2d_ensemble** out);
+int s2d_ensemble_destroy(s2d_ensemble* e);
+int s2d_ensemble_get_stream(s2d_ensemble* e, void** stream);
+int s2d_ensemble_synchronize(s2d_ensemble* e);
+/* Band-limited complex Gaussian initial spectra (kmin <= |k| <= kmax, rms
+ * vorticity `rms`) for every instance, seeded by the descriptor seeds. */
+int s2d_ensemble_seed_band(s2d_ensemble* e, float kmin, float kmax, float rms);
+int s2d_ensemble_set_state(s2d_ensemble* e, int index, const float* spectrum /* n*n*2 */);
+int s2d_ensemble_get_state(s2d_ensemble* e, int index, float* spectrum /* n*n*2 */);
+/* `steps` RK3 steps of every instance; use_graph replays a captured step. */
+int s2d_ensemble_step(s2d_ensemble* e, int steps, int use_graph);
+/* FP64 energy and enstrophy of every instance (arrays of `count`). */
+int s2d_ensemble_energy(s2d_ensemble* e, double* energy, double* enstrophy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* S2D_H */

@@ -1,0 +1,1050 @@
+// s2d_api.cu -- C ABI (include/s2d.h) over the sm_100a kernels.
+//
+// The solver object mirrors src/gpu/solver.js `class Solver`: it owns every
+// device buffer (the triple-buffered state ring, the FFT work buffers, the dye
+// textures as binary16 arrays) and one CUDA stream on which all of its work is
+// ordered, the way the reference encodes everything into one compute pass.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/s2d.h"
+#include "s2d_aux_kernels.cuh"
+#include "s2d_ops.cuh"
+
+using namespace s2d;
+
+static thread_local std::string g_last_error;
+
+static int fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+namespace s2d {
+// error text of the ensemble translation unit, reported by s2d_last_error()
+const char* ens_set_error(const std::string& m) {
+  g_last_error = m;
+  return g_last_error.c_str();
+}
+}  // namespace s2d
+#define S2D_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(S2D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+#define S2D_LAUNCHED()                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                                     \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(S2D_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_));    \
+  } while (0)
+
+// ------------------------------------------------------------------ size dispatch
+namespace s2d {
+const NOps* ops_n32();
+const NOps* ops_n64();
+const NOps* ops_n128();
+const NOps* ops_n256();
+const NOps* ops_n512();
+const NOps* ops_n1024();
+const NOps* ops_n2048();
+const NOps* ops_n4096();
+}  // namespace s2d
+
+static const NOps* ops_for(int n) {
+  switch (n) {
+    case 32: return ops_n32();
+    case 64: return ops_n64();
+    case 128: return ops_n128();
+    case 256: return ops_n256();
+    case 512: return ops_n512();
+    case 1024: return ops_n1024();
+    case 2048: return ops_n2048();
+    case 4096: return ops_n4096();
+    default: return nullptr;
+  }
+}
+
+static bool radix_ok(int n, int* stages, int* has_r2) {
+  if (n < 2) return false;
+  int s = 0, m = n;
+  while (m % 4 == 0) {
+    ++s;
+    m /= 4;
+  }
+  if (m != 1 && m != 2) return false;
+  if (stages) *stages = s;
+  if (has_r2) *has_r2 = (m == 2);
+  return true;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+static int check_device(int dev) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(S2D_ERR_NO_DEVICE, "no CUDA device available");
+  if (dev < 0 || dev >= count) return fail(S2D_ERR_ARG, "device index out of range");
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return fail(S2D_ERR_NO_DEVICE, "device query failed");
+  if (p.major != 10) return fail(S2D_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only");
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ solver object
+struct GraphKey {
+  int phase, slot, parity;
+  unsigned flags;
+  int ptr;
+  bool operator<(const GraphKey& o) const {
+    return std::tie(phase, slot, parity, flags, ptr) < std::tie(o.phase, o.slot, o.parity, o.flags, o.ptr);
+  }
+};
+
+struct s2d_solver {
+  int dev = 0, n = 0, m = 0, nbins = 0, dye_scale = 1, fft_precision = 0;
+  cudaStream_t stream = nullptr;
+  const NOps* ops = nullptr;
+  float2* state[3] = {nullptr, nullptr, nullptr};
+  float2 *packA = nullptr, *packB = nullptr, *physZ = nullptr, *rhs = nullptr, *force = nullptr,
+         *vel = nullptr, *tw = nullptr;
+  float* dtbuf = nullptr;      // 2 slots x [dt, speed]
+  float* partials = nullptr;
+  unsigned* ticket = nullptr;
+  DevParams* dparams = nullptr;
+  DevSplats* dsplats = nullptr;
+  double* diag = nullptr;      // nbins + 2
+  uint32_t* diag_fixed = nullptr;
+  float* zonal = nullptr;
+  double* seed_parts = nullptr;
+  uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
+  ushort4* dye[3] = {nullptr, nullptr, nullptr};
+  // pinned readback staging (copyDiagnostics)
+  double* h_diag = nullptr;
+  uint32_t* h_fixed = nullptr;
+  float* h_zonal = nullptr;
+  float* h_dt = nullptr;
+  cudaEvent_t diag_event = nullptr;
+  // host mirror of the JS Solver fields
+  DevParams hp{};
+  DevSplats hs{};
+  bool configured = false;
+  int phase = 0, dye_parity = 0, slot = 0;
+  uint32_t step_index = 0;
+  double sim_time = 0.0;
+  bool primed = false, packs_valid = false, reduced_valid = false, disposed = false;
+  int read_state = 0;  // 0 idle, 1 copied
+  std::map<GraphKey, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+  // instrumentation: event pairs around launches, by kernel class
+  bool profiling = false;
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> prof_events;
+};
+
+// RAII event pair around the launches of one kernel class (when profiling)
+struct ProfScope {
+  s2d_solver* s;
+  int cls;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(s2d_solver* s_, int c) : s(s_), cls(c) {
+    if (!s->profiling) return;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return;
+    cudaEventRecord(a, s->stream);
+  }
+  ~ProfScope() {
+    if (!a || !b) return;
+    cudaEventRecord(b, s->stream);
+    s->prof_events.emplace_back(cls, a, b);
+  }
+};
+
+static int seed_parts_count(int n) { return (n * n + 255) / 256; }
+
+static void free_solver(s2d_solver* s) {
+  for (auto& kv : s->graphs) {
+    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+  }
+  s->graphs.clear();
+  for (auto& ev : s->prof_events) {
+    cudaEventDestroy(std::get<1>(ev));
+    cudaEventDestroy(std::get<2>(ev));
+  }
+  s->prof_events.clear();
+  void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
+                      s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
+                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->dye[0], s->dye[1], s->dye[2]};
+  for (void* p : dev_ptrs)
+    if (p) cudaFree(p);
+  void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
+  for (void* p : host_ptrs)
+    if (p) cudaFreeHost(p);
+  if (s->diag_event) cudaEventDestroy(s->diag_event);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+#define S2D_USE(s)                                                         \
+  do {                                                                     \
+    if (!(s)) return fail(S2D_ERR_ARG, "null solver handle");              \
+    if ((s)->disposed) return fail(S2D_ERR_DESTROYED, "solver destroyed"); \
+  } while (0)
+
+// ------------------------------------------------------------------ library entry points
+extern "C" int s2d_version(void) { return 10000; }
+
+extern "C" const char* s2d_status_string(int st) {
+  switch (st) {
+    case S2D_OK: return "ok";
+    case S2D_NO_DATA: return "no data";
+    case S2D_ERR_ARG: return "bad argument";
+    case S2D_ERR_UNSUPPORTED_N: return "unsupported grid size";
+    case S2D_ERR_CUDA: return "CUDA error";
+    case S2D_ERR_DESTROYED: return "use after destroy";
+    case S2D_ERR_NAN: return "non-finite input";
+    case S2D_ERR_UNREGISTERED: return "buffer was never registered with the FFT";
+    case S2D_ERR_NO_DEVICE: return "no usable device";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* s2d_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int s2d_radix_schedule(int n, int* stages, int* has_radix2) {
+  if (!radix_ok(n, stages, has_radix2))
+    return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " must be 4^a or 2 * 4^a");
+  return S2D_OK;
+}
+
+extern "C" int s2d_supported_grids(int* out, int capacity, int* count) {
+  if (!count) return fail(S2D_ERR_ARG, "count is null");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(S2D_ERR_NO_DEVICE, "no CUDA device");
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  int c = 0;
+  for (int n = S2D_MIN_N; n <= S2D_MAX_N; n *= 2) {
+    const NOps* o = ops_for(n);
+    if (!o) continue;
+    const size_t need_smem = o->a_smem > o->b_smem ? o->a_smem : o->b_smem;
+    const size_t need_mem = (size_t)n * n * 8 * 10;   // 3 states, 6 work buffers, velocity
+    if (need_smem > (size_t)smem_optin || need_mem > total_b) continue;
+    if (out && c < capacity) out[c] = n;
+    ++c;
+  }
+  *count = c;
+  return S2D_OK;
+}
+
+static int table_prelude(int n) {
+  if (n < 2 || n > (1 << 16) || (n & (n - 1))) return fail(S2D_ERR_UNSUPPORTED_N, "size must be a power of two");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(S2D_ERR_NO_DEVICE, "no CUDA device");
+  return check_device(dev);
+}
+
+extern "C" int s2d_digit_reverse_table(int n, uint32_t* out) {
+  int st = 0, r2 = 0;
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  if (!radix_ok(n, &st, &r2)) return fail(S2D_ERR_UNSUPPORTED_N, "size must be 4^a or 2 * 4^a");
+  if (int rc = table_prelude(n)) return rc;
+  uint32_t* d = nullptr;
+  S2D_CUDA(cudaMalloc(&d, sizeof(uint32_t) * n));
+  k_digit_reverse<<<(n + 255) / 256, 256>>>(d, n, st, r2);
+  cudaError_t e = cudaMemcpy(out, d, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(S2D_ERR_CUDA, cudaGetErrorString(e));
+  return S2D_OK;
+}
+
+extern "C" int s2d_wavenumber_table(int n, float* out) {
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  if (int rc = table_prelude(n)) return rc;
+  float* d = nullptr;
+  S2D_CUDA(cudaMalloc(&d, sizeof(float) * n));
+  k_wavenumbers<<<(n + 255) / 256, 256>>>(d, n);
+  cudaError_t e = cudaMemcpy(out, d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(S2D_ERR_CUDA, cudaGetErrorString(e));
+  return S2D_OK;
+}
+
+extern "C" int s2d_dealias_mask_table(int n, uint8_t* out) {
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  if (int rc = table_prelude(n)) return rc;
+  uint8_t* d = nullptr;
+  const size_t cells = (size_t)n * n;
+  S2D_CUDA(cudaMalloc(&d, cells));
+  k_mask_table<<<(unsigned)((cells + 255) / 256), 256>>>(d, n);
+  cudaError_t e = cudaMemcpy(out, d, cells, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(S2D_ERR_CUDA, cudaGetErrorString(e));
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ lifecycle
+extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s2d_solver** out) {
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (!radix_ok(n, nullptr, nullptr) && !(n >= S2D_MIN_N && (n & (n - 1)) == 0))
+    return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " must be a power of two");
+  const NOps* ops = ops_for(n);
+  if (!ops) return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " outside 32..4096");
+  if (dye_scale < 1 || dye_scale > 4) return fail(S2D_ERR_ARG, "dye_scale must be 1..4");
+  if (fft_precision != S2D_FFT_FP32) return fail(S2D_ERR_ARG, "unknown FFT precision");
+  if (int rc = check_device(device)) return rc;
+  DeviceGuard guard(device);
+  s2d_solver* s = new s2d_solver();
+  s->dev = device;
+  s->n = n;
+  s->m = n * dye_scale;
+  s->dye_scale = dye_scale;
+  s->nbins = n / 2 + 1;
+  s->fft_precision = fft_precision;
+  s->ops = ops;
+  const size_t cbytes = (size_t)n * n * sizeof(float2);
+  const size_t dbytes = (size_t)s->m * s->m * sizeof(ushort4);
+  auto bail = [&](cudaError_t e, const char* what) {
+    free_solver(s);
+    delete s;
+    return fail(S2D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+#define TRY(call, what)            \
+  if ((e = (call)) != cudaSuccess) \
+    return bail(e, what);
+  TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  TRY(cudaEventCreateWithFlags(&s->diag_event, cudaEventDisableTiming), "event");
+  for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->state[i], cbytes), "state");
+  TRY(cudaMalloc(&s->packA, cbytes), "packA");
+  TRY(cudaMalloc(&s->packB, cbytes), "packB");
+  TRY(cudaMalloc(&s->physZ, cbytes), "physZ");
+  TRY(cudaMalloc(&s->rhs, cbytes), "rhs");
+  TRY(cudaMalloc(&s->force, cbytes), "force");
+  TRY(cudaMalloc(&s->vel, cbytes), "vel");
+  TRY(cudaMalloc(&s->tw, sizeof(float2) * n), "twiddles");
+  TRY(cudaMalloc(&s->dtbuf, sizeof(float) * 4), "dt");
+  const int nparts = std::max(std::max(ops->a_grid, 256), seed_parts_count(n));
+  TRY(cudaMalloc(&s->partials, sizeof(float) * nparts), "partials");
+  TRY(cudaMalloc(&s->ticket, sizeof(unsigned)), "ticket");
+  TRY(cudaMalloc(&s->dparams, sizeof(DevParams)), "params");
+  TRY(cudaMalloc(&s->dsplats, sizeof(DevSplats)), "splats");
+  TRY(cudaMalloc(&s->diag, sizeof(double) * (s->nbins + 2)), "diag");
+  TRY(cudaMalloc(&s->diag_fixed, sizeof(uint32_t) * (s->nbins + 2)), "diag fixed");
+  TRY(cudaMalloc(&s->zonal, sizeof(float) * n), "zonal");
+  TRY(cudaMalloc(&s->seed_parts, sizeof(double) * seed_parts_count(n)), "seed partials");
+  TRY(cudaMalloc(&s->step_counter, sizeof(uint32_t)), "step counter");
+  TRY(cudaMemsetAsync(s->step_counter, 0, sizeof(uint32_t), s->stream), "memset");
+  for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
+  TRY(cudaMallocHost(&s->h_diag, sizeof(double) * (s->nbins + 2)), "pinned diag");
+  TRY(cudaMallocHost(&s->h_fixed, sizeof(uint32_t) * (s->nbins + 2)), "pinned fixed");
+  TRY(cudaMallocHost(&s->h_zonal, sizeof(float) * n), "pinned zonal");
+  TRY(cudaMallocHost(&s->h_dt, sizeof(float) * 4), "pinned dt");
+  TRY(ops->set_attrs(), "kernel attributes");
+  // zero everything the reference's fresh buffers hold as zero
+  for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->packA, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->packB, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->physZ, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->rhs, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->force, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->vel, 0, cbytes, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->dtbuf, 0, sizeof(float) * 4, s->stream), "memset");
+  TRY(cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), s->stream), "memset");
+  TRY(cudaMemsetAsync(s->partials, 0, sizeof(float) * nparts, s->stream), "memset");
+  for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream), "memset");
+  k_twiddles<<<(n + 255) / 256, 256, 0, s->stream>>>(s->tw, n);
+  TRY(cudaGetLastError(), "twiddle kernel");
+  // an unconfigured solver has all-zero parameters apart from the grid constants
+  s->hp = DevParams{};
+  s->hp.n = n;
+  s->hp.kcut = (float)(n / 3.0);
+  s->hp.force_norm = (float)(0.01 * n * n);
+  s->hp.dx = (float)(2.0 * M_PI / n);
+  s->hs = DevSplats{};
+  TRY(cudaMemcpyAsync(s->dparams, &s->hp, sizeof(DevParams), cudaMemcpyHostToDevice, s->stream), "params");
+  TRY(cudaMemcpyAsync(s->dsplats, &s->hs, sizeof(DevSplats), cudaMemcpyHostToDevice, s->stream), "splats");
+  TRY(cudaStreamSynchronize(s->stream), "create sync");
+#undef TRY
+  *out = s;
+  return S2D_OK;
+}
+
+extern "C" int s2d_destroy(s2d_solver* s) {
+  if (!s) return fail(S2D_ERR_ARG, "null solver handle");
+  DeviceGuard guard(s->dev);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  s->disposed = true;
+  free_solver(s);
+  delete s;
+  return S2D_OK;
+}
+
+extern "C" int s2d_get_info(s2d_solver* s, s2d_info* out) {
+  S2D_USE(s);
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  out->n = s->n;
+  out->m = s->m;
+  out->nbins = s->nbins;
+  out->phase = s->phase;
+  out->dye_parity = s->dye_parity;
+  out->step_index = s->step_index;
+  out->primed = s->primed ? 1 : 0;
+  out->fft_precision = s->fft_precision;
+  out->nu_h = s->hp.nu_h;
+  out->sim_time = s->sim_time;
+  return S2D_OK;
+}
+
+extern "C" int s2d_set_phase(s2d_solver* s, int phase, int dye_parity) {
+  S2D_USE(s);
+  if (phase < 0 || phase > 2 || dye_parity < 0 || dye_parity > 1) return fail(S2D_ERR_ARG, "phase out of range");
+  if (phase != s->phase) s->packs_valid = false;
+  s->phase = phase;
+  s->dye_parity = dye_parity;
+  return S2D_OK;
+}
+
+extern "C" int s2d_set_sim_time(s2d_solver* s, double t) {
+  S2D_USE(s);
+  s->sim_time = t;
+  return S2D_OK;
+}
+
+extern "C" int s2d_get_stream(s2d_solver* s, void** stream) {
+  S2D_USE(s);
+  if (!stream) return fail(S2D_ERR_ARG, "out is null");
+  *stream = (void*)s->stream;
+  return S2D_OK;
+}
+
+extern "C" int s2d_synchronize(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ parameters
+extern "C" int s2d_configure(s2d_solver* s, const s2d_params* p) {
+  S2D_USE(s);
+  if (!p) return fail(S2D_ERR_ARG, "params is null");
+  if (p->hyper_p < 0 || p->hyper_p > 16) return fail(S2D_ERR_ARG, "hyperP must be in 0..16");
+  DeviceGuard guard(s->dev);
+  const double kcut = s->n / 3.0;
+  DevParams& h = s->hp;
+  h.beta = p->beta;
+  h.mu = p->drag;
+  h.nu_h = p->viscosity > 0 ? (float)(p->viscosity / std::pow(kcut, 2.0 * p->hyper_p)) : 0.f;
+  h.hyper_p = p->hyper_p;
+  h.force_amp = p->force_amp;
+  h.force_k = p->force_k;
+  h.force_width = p->force_width;
+  h.step_index = s->step_index;    // latched once per configure (solver.js:316)
+  h.dx = (float)(2.0 * M_PI / s->n);
+  h.cfl = p->cfl;
+  h.dt_min = p->dt_min;
+  h.dt_max = p->dt_max;
+  h.dye_fade = p->dye_fade;
+  h.kcut = (float)kcut;
+  h.force_norm = (float)(0.01 * s->n * s->n);
+  h.n = s->n;
+  S2D_CUDA(cudaMemcpyAsync(s->dparams, &h, sizeof(DevParams), cudaMemcpyHostToDevice, s->stream));
+  s->configured = true;
+  return S2D_OK;
+}
+
+extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
+  S2D_USE(s);
+  if (count < 0 || (count > 0 && !list)) return fail(S2D_ERR_ARG, "bad splat list");
+  DeviceGuard guard(s->dev);
+  const int c = count < S2D_MAX_SPLATS ? count : S2D_MAX_SPLATS;   // Math.min (solver.js:327)
+  s->hs = DevSplats{};
+  s->hs.count = c;
+  for (int i = 0; i < c; ++i) {
+    const s2d_splat& a = list[i];
+    DevSplat& d = s->hs.items[i];
+    d.x = a.x; d.y = a.y; d.vx = a.dx; d.vy = a.dy;
+    d.r = a.color[0]; d.g = a.color[1]; d.b = a.color[2];
+    d.radius = a.radius; d.amp = a.amp; d.dye_amp = a.dye_amp;
+  }
+  S2D_CUDA(cudaMemcpyAsync(s->dsplats, &s->hs, sizeof(DevSplats), cudaMemcpyHostToDevice, s->stream));
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ internal enqueue helpers
+static inline unsigned cells_grid(int n) { return (unsigned)(((size_t)n * n + 255) / 256); }
+
+static int enqueue_fft2(s2d_solver* s, float2* buf, int sign) {
+  s->ops->fft_rows(sign, buf, s->tw, s->stream);
+  S2D_LAUNCHED();
+  s->ops->fft_cols(sign, buf, s->tw, s->stream);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+static float* dt_slot(s2d_solver* s, int slot) { return s->dtbuf + 2 * slot; }
+
+// prime packs from state[phase]: PA/PB = FFT_x^-1 of the scaled packs
+static int enqueue_pack_prime(s2d_solver* s) {
+  SpecArgs a{};
+  a.wcur = s->state[s->phase];
+  a.pa = s->packA;
+  a.pb = s->packB;
+  a.dt = dt_slot(s, s->slot);
+  a.params = s->dparams;
+  a.tw = s->tw;
+  s->ops->spec_rows(-1, false, a, s->stream);
+  S2D_LAUNCHED();
+  s->packs_valid = true;
+  return S2D_OK;
+}
+
+static PhysArgs phys_args(s2d_solver* s, int reduce) {
+  PhysArgs a{};
+  a.pa = s->packA;
+  a.pb = s->packB;
+  a.z = s->physZ;
+  a.vel = s->vel;
+  a.partials = s->partials;
+  a.ticket = s->ticket;
+  a.dt_out = dt_slot(s, s->slot ^ 1);
+  a.params = s->dparams;
+  a.tw = s->tw;
+  a.reduce = reduce;
+  return a;
+}
+
+extern "C" int s2d_encode_reduce(s2d_solver* s);
+
+extern "C" int s2d_encode_prime(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  if (int rc = enqueue_pack_prime(s)) return rc;
+  PhysArgs a = phys_args(s, 1);
+  s->ops->phys_cols(0, a, s->stream);
+  S2D_LAUNCHED();
+  s->reduced_valid = true;
+  if (int rc = s2d_encode_reduce(s)) return rc;
+  s->primed = true;
+  return S2D_OK;
+}
+
+extern "C" int s2d_encode_step(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  if (!s->packs_valid)
+    if (int rc = enqueue_pack_prime(s)) return rc;
+  const bool ptr = s->hs.count > 0;
+  if (ptr) {
+    ProfScope ps(s, S2D_PROF_FORCE);
+    k_pointer_force<<<cells_grid(s->n), 256, 0, s->stream>>>(s->force, s->dsplats, s->n);
+    S2D_LAUNCHED();
+    if (int rc = enqueue_fft2(s, s->force, -1)) return rc;
+  }
+  const int p = s->phase;
+  for (int st = 0; st < 3; ++st) {
+    {
+      ProfScope ps(s, S2D_PROF_PHYS_COLS);
+      PhysArgs pa = phys_args(s, st == 2 ? 1 : 0);
+      s->ops->phys_cols(st == 2 ? 2 : 1, pa, s->stream);
+      S2D_LAUNCHED();
+    }
+    ProfScope ps(s, S2D_PROF_SPEC_ROWS);
+    SpecArgs a{};
+    a.z = s->physZ;
+    a.w0 = s->state[p];
+    a.wcur = s->state[(p + st) % 3];
+    a.wout = s->state[(p + (st == 1 ? 2 : 1)) % 3];
+    a.fptr = ptr ? s->force : nullptr;
+    a.pa = s->packA;
+    a.pb = s->packB;
+    a.dt = dt_slot(s, s->slot);
+    a.params = s->dparams;
+    a.tw = s->tw;
+    a.stochastic = s->hp.force_amp > 0.f ? 1 : 0;
+    s->ops->spec_rows(st, ptr, a, s->stream);
+    S2D_LAUNCHED();
+  }
+  s->reduced_valid = true;
+  s->packs_valid = true;
+  s->phase = (p + 1) % 3;
+  s->step_index += 1;
+  return S2D_OK;
+}
+
+extern "C" int s2d_encode_dye(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  const int p = s->dye_parity, m = s->m;
+  const dim3 blk(16, 16), grd((m + 15) / 16, (m + 15) / 16);
+  const float* dt = dt_slot(s, s->slot);
+  ProfScope ps(s, S2D_PROF_DYE);
+  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[p], s->dye[1 - p], dt, 1.f, s->n, m);
+  S2D_LAUNCHED();
+  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[1 - p], s->dye[2], dt, -1.f, s->n, m);
+  S2D_LAUNCHED();
+  k_dye_correct<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[p], s->dye[2], s->dye[1 - p], dt, s->dparams,
+                                            s->dsplats, s->n, m);
+  S2D_LAUNCHED();
+  s->dye_parity = 1 - p;
+  return S2D_OK;
+}
+
+extern "C" int s2d_encode_reduce(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  if (!s->reduced_valid) {
+    // velocity came from a stage hook: the reference's two-level reduction
+    const int groups = 256;
+    k_reduce_speed<<<groups, 256, 0, s->stream>>>(s->vel, s->partials, s->n * s->n);
+    S2D_LAUNCHED();
+    k_reduce_dt<<<1, 256, 0, s->stream>>>(s->partials, groups, dt_slot(s, s->slot ^ 1), s->dparams);
+    S2D_LAUNCHED();
+  }
+  s->slot ^= 1;
+  s->reduced_valid = false;
+  return S2D_OK;
+}
+
+static int sync_step_counter(s2d_solver* s) {
+  const uint32_t v = s->step_index;   // pageable source: staged before the call returns
+  S2D_CUDA(cudaMemcpyAsync(s->step_counter, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+  return S2D_OK;
+}
+
+static int enqueue_relatch(s2d_solver* s) {
+  k_latch_step<<<1, 1, 0, s->stream>>>(s->dparams, s->step_counter);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+extern "C" int s2d_step(s2d_solver* s, int substeps, unsigned flags) {
+  S2D_USE(s);
+  if (substeps < 0) return fail(S2D_ERR_ARG, "substeps < 0");
+  DeviceGuard guard(s->dev);
+  if (!s->primed)
+    if (int rc = s2d_encode_prime(s)) return rc;
+  if (flags & S2D_STEP_RELATCH)
+    if (int rc = sync_step_counter(s)) return rc;
+  for (int i = 0; i < substeps; ++i) {
+    if (flags & S2D_STEP_RELATCH)
+      if (int rc = enqueue_relatch(s)) return rc;
+    if (int rc = s2d_encode_step(s)) return rc;
+    if (flags & S2D_STEP_DYE)
+      if (int rc = s2d_encode_dye(s)) return rc;
+    if (flags & S2D_STEP_REDUCE)
+      if (int rc = s2d_encode_reduce(s)) return rc;
+  }
+  return S2D_OK;
+}
+
+extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
+  S2D_USE(s);
+  if (substeps < 0) return fail(S2D_ERR_ARG, "substeps < 0");
+  DeviceGuard guard(s->dev);
+  if (!s->primed)
+    if (int rc = s2d_encode_prime(s)) return rc;
+  if (!s->packs_valid)
+    if (int rc = enqueue_pack_prime(s)) return rc;
+  if (flags & S2D_STEP_RELATCH)
+    if (int rc = sync_step_counter(s)) return rc;
+  for (int i = 0; i < substeps; ++i) {
+    const GraphKey key{s->phase, s->slot, s->dye_parity, flags, s->hs.count > 0 ? 1 : 0};
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+      // capture one substep from the current host state, then restore it
+      const int phase = s->phase, slot = s->slot, parity = s->dye_parity;
+      const uint32_t si = s->step_index;
+      const bool rv = s->reduced_valid;
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t ge = nullptr;
+      S2D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = (flags & S2D_STEP_RELATCH) ? enqueue_relatch(s) : S2D_OK;
+      if (!rc) rc = s2d_encode_step(s);
+      if (!rc && (flags & S2D_STEP_DYE)) rc = s2d_encode_dye(s);
+      if (!rc && (flags & S2D_STEP_REDUCE)) rc = s2d_encode_reduce(s);
+      cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail(S2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&ge, g, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(S2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      }
+      s->phase = phase;
+      s->slot = slot;
+      s->dye_parity = parity;
+      s->step_index = si;
+      s->reduced_valid = rv;
+      it = s->graphs.emplace(key, std::make_pair(g, ge)).first;
+    }
+    S2D_CUDA(cudaGraphLaunch(it->second.second, s->stream));
+    // advance the host mirror exactly as the captured substep did
+    s->phase = (s->phase + 1) % 3;
+    s->step_index += 1;
+    s->packs_valid = true;
+    s->reduced_valid = true;
+    if (flags & S2D_STEP_DYE) s->dye_parity ^= 1;
+    if (flags & S2D_STEP_REDUCE) {
+      s->slot ^= 1;
+      s->reduced_valid = false;
+    }
+  }
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ diagnostics
+extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  const int n = s->n, nb = s->nbins;
+  S2D_CUDA(cudaMemsetAsync(s->diag, 0, sizeof(double) * (nb + 2), s->stream));
+  S2D_CUDA(cudaMemsetAsync(s->diag_fixed, 0, sizeof(uint32_t) * (nb + 2), s->stream));
+  const unsigned blocks = std::min<unsigned>(cells_grid(n), 148u * 4u);
+  k_diag_spectrum<<<blocks, 256, sizeof(double) * (nb + 2), s->stream>>>(s->state[s->phase], s->diag, n);
+  S2D_LAUNCHED();
+  k_diag_fixed<<<cells_grid(n), 256, 0, s->stream>>>(s->state[s->phase], s->diag_fixed, n);
+  S2D_LAUNCHED();
+  k_zonal_mean<<<n, 128, 0, s->stream>>>(s->vel, s->zonal, n);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
+  S2D_USE(s);
+  if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
+  DeviceGuard guard(s->dev);
+  const int nb = s->nbins;
+  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, sizeof(double) * (nb + 2), cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaMemcpyAsync(s->h_fixed, s->diag_fixed, sizeof(uint32_t) * (nb + 2), cudaMemcpyDeviceToHost,
+                           s->stream));
+  S2D_CUDA(cudaMemcpyAsync(s->h_zonal, s->zonal, sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), sizeof(float) * 2, cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaEventRecord(s->diag_event, s->stream));
+  s->read_state = 1;
+  return S2D_OK;
+}
+
+extern "C" int s2d_poll_diagnostics(s2d_solver* s) {
+  S2D_USE(s);
+  if (s->read_state != 1) return 0;
+  return cudaEventQuery(s->diag_event) == cudaSuccess ? 1 : 0;
+}
+
+extern "C" int s2d_read_diagnostics(s2d_solver* s, double* spectrum, float* zonal, double* energy,
+                                    double* enstrophy, float* dt, float* max_speed) {
+  S2D_USE(s);
+  if (s->read_state != 1) return S2D_NO_DATA;
+  DeviceGuard guard(s->dev);
+  cudaError_t e = cudaEventSynchronize(s->diag_event);
+  s->read_state = 0;
+  if (e != cudaSuccess) return fail(S2D_ERR_CUDA, cudaGetErrorString(e));
+  const int nb = s->nbins;
+  if (spectrum) std::memcpy(spectrum, s->h_diag, sizeof(double) * nb);
+  if (zonal) std::memcpy(zonal, s->h_zonal, sizeof(float) * s->n);
+  if (energy) *energy = s->h_diag[nb];
+  if (enstrophy) *enstrophy = s->h_diag[nb + 1];
+  if (dt) *dt = s->h_dt[0];
+  if (max_speed) *max_speed = s->h_dt[1];
+  return S2D_OK;
+}
+
+extern "C" int s2d_read_diagnostics_fixed(s2d_solver* s, float* spectrum, float* energy, float* enstrophy) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaEventSynchronize(s->diag_event));
+  const int nb = s->nbins;
+  if (spectrum)
+    for (int i = 0; i < nb; ++i) spectrum[i] = (float)(s->h_fixed[i] / 1e8);
+  if (energy) *energy = (float)(s->h_fixed[nb] / 1e6);
+  if (enstrophy) *enstrophy = (float)(s->h_fixed[nb + 1] / 1e6);
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ seeding
+static int zero_other_states(s2d_solver* s) {
+  const size_t cbytes = (size_t)s->n * s->n * sizeof(float2);
+  S2D_CUDA(cudaMemsetAsync(s->state[1], 0, cbytes, s->stream));
+  S2D_CUDA(cudaMemsetAsync(s->state[2], 0, cbytes, s->stream));
+  return S2D_OK;
+}
+
+extern "C" int s2d_seed(s2d_solver* s, double k0, double amplitude, uint32_t seed) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  const int n = s->n;
+  const size_t cbytes = (size_t)n * n * sizeof(float2);
+  if (amplitude > 0) {
+    const int parts = seed_parts_count(n);
+    k_fill_spectrum<<<parts, 256, 0, s->stream>>>(s->state[0], s->seed_parts, n, k0, hash1(seed));
+    S2D_LAUNCHED();
+    k_scale_spectrum<<<std::min(parts, 1024), 256, 0, s->stream>>>(s->state[0], s->seed_parts, parts, n,
+                                                                    amplitude);
+    S2D_LAUNCHED();
+  } else {
+    S2D_CUDA(cudaMemsetAsync(s->state[0], 0, cbytes, s->stream));
+  }
+  s->phase = 0;
+  s->packs_valid = false;
+  return zero_other_states(s);
+}
+
+extern "C" int s2d_seed_band(s2d_solver* s, float kmin, float kmax, float rms, uint32_t seed) {
+  S2D_USE(s);
+  if (!(rms >= 0.f) || !(kmax >= kmin)) return fail(S2D_ERR_ARG, "bad band or rms");
+  DeviceGuard guard(s->dev);
+  const int n = s->n, parts = seed_parts_count(n);
+  k_band_seed<<<parts, 256, 0, s->stream>>>(s->state[0], s->seed_parts, n, kmin, kmax, seed);
+  S2D_LAUNCHED();
+  k_scale_spectrum<<<std::min(parts, 1024), 256, 0, s->stream>>>(s->state[0], s->seed_parts, parts, n, rms);
+  S2D_LAUNCHED();
+  s->phase = 0;
+  s->packs_valid = false;
+  return zero_other_states(s);
+}
+
+static int check_finite(const float* v, size_t count) {
+  for (size_t i = 0; i < count; ++i)
+    if (!std::isfinite(v[i])) return fail(S2D_ERR_NAN, "non-finite value at index " + std::to_string(i));
+  return S2D_OK;
+}
+
+extern "C" int s2d_seed_physical(s2d_solver* s, const float* field) {
+  S2D_USE(s);
+  if (!field) return fail(S2D_ERR_ARG, "field is null");
+  const int n = s->n;
+  if (int rc = check_finite(field, (size_t)n * n)) return rc;
+  DeviceGuard guard(s->dev);
+  // stage the real field in the velocity buffer, then packA = (field, 0)
+  float* staging = reinterpret_cast<float*>(s->vel);
+  S2D_CUDA(cudaMemcpyAsync(staging, field, sizeof(float) * n * n, cudaMemcpyHostToDevice, s->stream));
+  k_real_to_complex<<<cells_grid(n), 256, 0, s->stream>>>(staging, s->packA, n * n);
+  S2D_LAUNCHED();
+  if (int rc = enqueue_fft2(s, s->packA, -1)) return rc;
+  k_seed_mask<<<cells_grid(n), 256, 0, s->stream>>>(s->packA, s->state[0], n);
+  S2D_LAUNCHED();
+  S2D_CUDA(cudaStreamSynchronize(s->stream));   // the host field must outlive the copy
+  s->phase = 0;
+  s->packs_valid = false;
+  s->reduced_valid = false;
+  return zero_other_states(s);
+}
+
+extern "C" int s2d_paint_dye(s2d_solver* s, int pattern) {
+  S2D_USE(s);
+  if (pattern == S2D_DYE_NONE) return S2D_OK;
+  if (pattern != S2D_DYE_BANDS) return fail(S2D_ERR_ARG, "unknown dye pattern");
+  DeviceGuard guard(s->dev);
+  const int m = s->m;
+  k_paint_bands<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, s->stream>>>(s->dye[s->dye_parity], m);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+extern "C" int s2d_reset(s2d_solver* s, const float* field, double k0, double amplitude, uint32_t seed,
+                         int dye_pattern) {
+  S2D_USE(s);
+  if (dye_pattern != S2D_DYE_NONE && dye_pattern != S2D_DYE_BANDS) return fail(S2D_ERR_ARG, "unknown dye pattern");
+  DeviceGuard guard(s->dev);
+  s->step_index = 0;
+  s->sim_time = 0.0;
+  s->dye_parity = 0;
+  int rc = field ? s2d_seed_physical(s, field) : s2d_seed(s, k0, amplitude, seed);
+  if (rc) return rc;
+  const size_t dbytes = (size_t)s->m * s->m * sizeof(ushort4);
+  for (int i = 0; i < 3; ++i) S2D_CUDA(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream));
+  if ((rc = s2d_paint_dye(s, dye_pattern))) return rc;
+  const float dt0[2] = {s->configured ? s->hp.dt_max : 0.01f, 0.f};
+  S2D_CUDA(cudaMemcpyAsync(dt_slot(s, s->slot), dt0, sizeof(dt0), cudaMemcpyHostToDevice, s->stream));
+  S2D_CUDA(cudaMemsetAsync(s->force, 0, (size_t)s->n * s->n * sizeof(float2), s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  s->primed = false;
+  s->packs_valid = false;
+  s->reduced_valid = false;
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ stage hooks
+static int buffer_for(s2d_solver* s, int id, void** ptr, size_t* bytes) {
+  const size_t cbytes = (size_t)s->n * s->n * sizeof(float2);
+  switch (id) {
+    case S2D_BUF_STATE0: case S2D_BUF_STATE1: case S2D_BUF_STATE2: *ptr = s->state[id]; *bytes = cbytes; return 0;
+    case S2D_BUF_PACKA: *ptr = s->packA; *bytes = cbytes; return 0;
+    case S2D_BUF_PACKB: *ptr = s->packB; *bytes = cbytes; return 0;
+    case S2D_BUF_PHYSZ: *ptr = s->physZ; *bytes = cbytes; return 0;
+    case S2D_BUF_RHS: *ptr = s->rhs; *bytes = cbytes; return 0;
+    case S2D_BUF_FORCE: *ptr = s->force; *bytes = cbytes; return 0;
+    case S2D_BUF_VEL: *ptr = s->vel; *bytes = cbytes; return 0;
+    case S2D_BUF_DT: *ptr = dt_slot(s, s->slot); *bytes = 2 * sizeof(float); return 0;
+    default: return fail(S2D_ERR_ARG, "unknown buffer id " + std::to_string(id));
+  }
+}
+
+extern "C" int s2d_get_buffer(s2d_solver* s, int id, void* host, size_t bytes) {
+  S2D_USE(s);
+  if (!host) return fail(S2D_ERR_ARG, "host is null");
+  void* p = nullptr;
+  size_t sz = 0;
+  if (int rc = buffer_for(s, id, &p, &sz)) return rc;
+  DeviceGuard guard(s->dev);
+  if (id == S2D_BUF_DT) {
+    if (bytes < sz) return fail(S2D_ERR_ARG, "host buffer too small");
+    float tmp[4] = {0, 0, 0, 0};
+    S2D_CUDA(cudaMemcpyAsync(tmp, p, sz, cudaMemcpyDeviceToHost, s->stream));
+    S2D_CUDA(cudaStreamSynchronize(s->stream));
+    std::memcpy(host, tmp, std::min(bytes, sizeof(tmp)));
+    return S2D_OK;
+  }
+  if (bytes > sz) return fail(S2D_ERR_ARG, "requested more bytes than the buffer holds");
+  S2D_CUDA(cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
+}
+
+extern "C" int s2d_set_buffer(s2d_solver* s, int id, const void* host, size_t bytes) {
+  S2D_USE(s);
+  if (!host) return fail(S2D_ERR_ARG, "host is null");
+  void* p = nullptr;
+  size_t sz = 0;
+  if (int rc = buffer_for(s, id, &p, &sz)) return rc;
+  if (id == S2D_BUF_DT) bytes = std::min(bytes, sz);
+  if (bytes > sz) return fail(S2D_ERR_ARG, "more bytes than the buffer holds");
+  if (int rc = check_finite(static_cast<const float*>(host), bytes / sizeof(float))) return rc;
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  if (id <= S2D_BUF_PACKB) s->packs_valid = false;
+  if (id == S2D_BUF_VEL) s->reduced_valid = false;
+  return S2D_OK;
+}
+
+extern "C" int s2d_fft2(s2d_solver* s, int id, int inverse) {
+  S2D_USE(s);
+  float2* buf = nullptr;
+  switch (id) {   // the buffers Solver.build registers (solver.js:133-136)
+    case S2D_BUF_PACKA: buf = s->packA; break;
+    case S2D_BUF_PACKB: buf = s->packB; break;
+    case S2D_BUF_PHYSZ: buf = s->physZ; break;
+    case S2D_BUF_FORCE: buf = s->force; break;
+    default: return fail(S2D_ERR_UNREGISTERED, "buffer " + std::to_string(id) + " was never registered with the FFT");
+  }
+  DeviceGuard guard(s->dev);
+  if (id == S2D_BUF_PACKA || id == S2D_BUF_PACKB) s->packs_valid = false;
+  return enqueue_fft2(s, buf, inverse ? +1 : -1);
+}
+
+extern "C" int s2d_velocity_pack(s2d_solver* s, int state_index) {
+  S2D_USE(s);
+  if (state_index < 0 || state_index > 2) return fail(S2D_ERR_ARG, "state index out of range");
+  DeviceGuard guard(s->dev);
+  k_velocity_pack<<<cells_grid(s->n), 256, 0, s->stream>>>(s->state[state_index], s->packA, s->packB, s->n);
+  S2D_LAUNCHED();
+  s->packs_valid = false;
+  return S2D_OK;
+}
+
+extern "C" int s2d_nl_pack(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  k_nl_pack<<<cells_grid(s->n), 256, 0, s->stream>>>(s->packA, s->packB, s->physZ, s->vel, s->n);
+  S2D_LAUNCHED();
+  s->reduced_valid = false;
+  return S2D_OK;
+}
+
+extern "C" int s2d_assemble(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  k_assemble<<<cells_grid(s->n), 256, 0, s->stream>>>(s->physZ, s->force, dt_slot(s, s->slot), s->dparams,
+                                                      s->rhs, s->n);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+extern "C" int s2d_rk3_stage(s2d_solver* s, int stage) {
+  S2D_USE(s);
+  if (stage < 0 || stage > 2) return fail(S2D_ERR_ARG, "stage out of range");
+  DeviceGuard guard(s->dev);
+  const int p = s->phase;
+  float2* w0 = s->state[p];
+  float2* wc = s->state[(p + stage) % 3];
+  float2* wo = s->state[(p + (stage == 1 ? 2 : 1)) % 3];
+  const float* dt = dt_slot(s, s->slot);
+  const unsigned g = cells_grid(s->n);
+  if (stage == 0) k_rk3<0><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+  else if (stage == 1) k_rk3<1><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+  else k_rk3<2><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+  S2D_LAUNCHED();
+  s->packs_valid = false;
+  return S2D_OK;
+}
+
+extern "C" int s2d_get_dye(s2d_solver* s, uint16_t* out) {
+  S2D_USE(s);
+  if (!out) return fail(S2D_ERR_ARG, "out is null");
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaMemcpyAsync(out, s->dye[s->dye_parity], (size_t)s->m * s->m * sizeof(ushort4),
+                           cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
+}
+
+extern "C" int s2d_set_dye(s2d_solver* s, const uint16_t* in) {
+  S2D_USE(s);
+  if (!in) return fail(S2D_ERR_ARG, "in is null");
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaMemcpyAsync(s->dye[s->dye_parity], in, (size_t)s->m * s->m * sizeof(ushort4),
+                           cudaMemcpyHostToDevice, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ instrumentation
+extern "C" int s2d_profile(s2d_solver* s, int enable) {
+  S2D_USE(s);
+  s->profiling = enable != 0;
+  return S2D_OK;
+}
+
+extern "C" int s2d_profile_read(s2d_solver* s, double* ms, int* launches) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  double acc[S2D_PROF_CLASSES] = {0};
+  int cnt[S2D_PROF_CLASSES] = {0};
+  for (auto& ev : s->prof_events) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, std::get<1>(ev), std::get<2>(ev)) == cudaSuccess) {
+      acc[std::get<0>(ev)] += t;
+      cnt[std::get<0>(ev)] += 1;
+    }
+    cudaEventDestroy(std::get<1>(ev));
+    cudaEventDestroy(std::get<2>(ev));
+  }
+  s->prof_events.clear();
+  for (int i = 0; i < S2D_PROF_CLASSES; ++i) {
+    if (ms) ms[i] = acc[i];
+    if (launches) launches[i] = cnt[i];
+  }
+  return S2D_OK;
+}

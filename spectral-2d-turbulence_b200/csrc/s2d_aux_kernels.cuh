@@ -1,0 +1,434 @@
+// s2d_aux_kernels.cuh -- forcing, CFL reduction, diagnostics, seeding, dye, tables.
+#pragma once
+#include <cuda_fp16.h>
+#include "s2d_band.cuh"
+#include "s2d_device.cuh"
+
+namespace s2d {
+
+// ------------------------------------------------------------------ tables (FP64 generation)
+// exp(-2 pi i m / n) for m < n, generated in FP64 and rounded once to float.
+__global__ void k_twiddles(float2* tw, int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  double s, c;
+  sincospi(2.0 * (double)m / (double)n, &s, &c);
+  tw[m] = make_float2((float)c, (float)(-s));
+}
+
+// digit reversal over the reversed radix list [4,..,4,(2)] (fft.wgsl:32-40, fft_ref.py:19-24)
+__global__ void k_digit_reverse(uint32_t* out, int n, int stages, int has_r2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t v = (uint32_t)i, o = 0;
+  if (has_r2) {
+    o = o * 2u + (v % 2u);
+    v /= 2u;
+  }
+  for (int s = 0; s < stages; ++s) {
+    o = o * 4u + (v % 4u);
+    v /= 4u;
+  }
+  out[i] = o;
+}
+
+__global__ void k_wavenumbers(float* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = wn_rt(i, n);
+}
+
+__global__ void k_mask_table(uint8_t* out, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float kcut = (float)(n / 3.0);
+  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
+  out[idx] = (fabsf(kx) < kcut && fabsf(ky) < kcut) ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ pointer forcing (force.wgsl:5-27)
+__device__ __forceinline__ float wrap01(float x) { return x - floorf(x); }
+__device__ __forceinline__ float sepf(float a, float b) { return wrap01(a - b + 0.5f) - 0.5f; }
+
+__global__ void k_pointer_force(float2* force, const DevSplats* __restrict__ S, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float nf = (float)n;
+  const float x = ((float)(idx & (n - 1)) + 0.5f) / nf;
+  const float y = ((float)(idx / n) + 0.5f) / nf;
+  float total = 0.f;
+  const int cnt = S->count;
+  for (int i = 0; i < cnt; ++i) {
+    const DevSplat s = S->items[i];
+    const float rx = sepf(x, s.x), ry = sepf(y, s.y);
+    const float r2 = rx * rx + ry * ry;
+    const float sig2 = fmaxf(s.radius * s.radius, 1e-8f);
+    if (r2 < 9.f * sig2) {
+      const float g = expf(-r2 / sig2);
+      total += 2.f * s.amp * g * (s.vx * ry - s.vy * rx) / sig2;
+    }
+  }
+  force[idx] = make_float2(total, 0.f);
+}
+
+// params.step_index = counter++ (one thread): the step index a configure() before
+// this substep would latch (solver.js:316)
+__global__ void k_latch_step(DevParams* params, uint32_t* counter) {
+  const uint32_t k = *counter;
+  params->step_index = k;
+  *counter = k + 1u;
+}
+
+// ------------------------------------------------------------------ CFL reduction (reduce.wgsl:22-63)
+__global__ void k_reduce_speed(const float2* __restrict__ vel, float* partials, int ncells) {
+  float m = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncells; i += gridDim.x * blockDim.x) {
+    const float2 v = vel[i];
+    m = fmaxf(m, fabsf(v.x) + fabsf(v.y));
+  }
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.f;
+    s = warp_max(s);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  }
+}
+
+__global__ void k_reduce_dt(const float* __restrict__ partials, int count, float* dt_out,
+                            const DevParams* __restrict__ params) {
+  float m = 0.f;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) m = fmaxf(m, partials[i]);
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.f;
+    s = warp_max(s);
+    if (threadIdx.x == 0) {
+      dt_out[0] = cfl_dt(*params, s);
+      dt_out[1] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ seeding
+// seed.wgsl:4-17: dst = src * mask, k = 0 cleared
+__global__ void k_seed_mask(const float2* __restrict__ src, float2* dst, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float kcut = (float)(n / 3.0);
+  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
+  if (kx == 0.f && ky == 0.f) {
+    dst[idx] = make_float2(0.f, 0.f);
+    return;
+  }
+  dst[idx] = (fabsf(kx) < kcut && fabsf(ky) < kcut) ? src[idx] : make_float2(0.f, 0.f);
+}
+
+// real field -> complex (value, 0) (solver.js:363-367)
+__global__ void k_real_to_complex(const float* __restrict__ src, float2* dst, int ncells) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ncells) dst[i] = make_float2(src[i], 0.f);
+}
+
+// fillSpectrum (solver.js:384-418) in double precision like the JS host code:
+// unscaled Float32 values plus per-CTA partial sums of amp^2.
+__global__ void k_fill_spectrum(float2* data, double* partial, int n, double k0, uint32_t salt) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  if (idx < n * n) {
+    const int col = idx & (n - 1), row = idx / n;
+    const double kcut = n / 3.0;
+    const int kxi = col < n / 2 ? col : col - n;
+    const int kyi = row < n / 2 ? row : row - n;
+    float2 val = make_float2(0.f, 0.f);
+    if (!((kxi == 0 && kyi == 0) || abs(kxi) >= kcut || abs(kyi) >= kcut)) {
+      const double kr = hypot((double)kxi, (double)kyi);
+      const double q = kr / k0;
+      const double q2 = q * q, q4 = q2 * q2;
+      const double env = kr * kr / (1.0 + q4 * q4);
+      const double amp = sqrt(env);
+      const bool canon = kyi > 0 || (kyi == 0 && kxi > 0);
+      const int hr = canon ? row : (n - row) % n;
+      const int hc = canon ? col : (n - col) % n;
+      const double sgn = canon ? 1.0 : -1.0;
+      const double phase = 2.0 * 3.14159265358979323846 * (double)hash1((uint32_t)(hr * n + hc) ^ salt) / 4294967296.0;
+      double s, c;
+      sincos(phase, &s, &c);
+      val = make_float2((float)(amp * c), (float)(sgn * amp * s));
+      acc = amp * amp;
+    }
+    data[idx] = val;
+  }
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// band-limited Gaussian spectrum (s2d_band.cuh) with per-CTA partial sums of |w|^2
+__global__ void k_band_seed(float2* data, double* partial, int n, float kmin, float kmax, uint32_t seed) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  if (idx < n * n) {
+    const float2 v = band_cell(seed, n, idx / n, idx & (n - 1), kmin, kmax);
+    data[idx] = v;
+    acc = (double)v.x * v.x + (double)v.y * v.y;
+  }
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// scale = amplitude / (sqrt(sum)/n^2); data *= scale (Float32Array *= double, solver.js:411-417)
+__global__ void k_scale_spectrum(float2* data, const double* partial, int nparts, int n, double amplitude) {
+  __shared__ double scale;
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int i = 0; i < nparts; ++i) sum += partial[i];
+    const double rms = sqrt(sum) / ((double)n * (double)n);
+    scale = rms > 0.0 ? amplitude / rms : 1.0;
+  }
+  __syncthreads();
+  const double sc = scale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x) {
+    const float2 v = data[i];
+    data[i] = make_float2((float)((double)v.x * sc), (float)((double)v.y * sc));
+  }
+}
+
+// ------------------------------------------------------------------ diagnostics
+// FP64 energy, enstrophy and radial spectrum of the state (spectral2d.py:92-104):
+// per-CTA shared histograms in double, one atomicAdd per bin per CTA.
+// out[0..nbins) spectrum, out[nbins] energy, out[nbins+1] enstrophy.
+__global__ void k_diag_spectrum(const float2* __restrict__ w, double* out, int n) {
+  extern __shared__ double hist[];
+  const int nb = n / 2 + 1;
+  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) hist[i] = 0.0;
+  __syncthreads();
+  const double n4 = (double)n * n * (double)n * n;
+  double ene = 0.0, ens = 0.0;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+    const int kx = (idx & (n - 1)) < n / 2 ? (idx & (n - 1)) : (idx & (n - 1)) - n;
+    const int row = idx / n;
+    const int ky = row < n / 2 ? row : row - n;
+    const double k2 = (double)kx * kx + (double)ky * ky;
+    const float2 a = w[idx];
+    const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) / n4;
+    ens += z;
+    if (k2 > 0.0) {
+      const double e = z / k2;
+      ene += e;
+      int b = (int)floor(sqrt(k2) + 0.5);
+      b = b < nb - 1 ? b : nb - 1;
+      atomicAdd(&hist[b], e);
+    }
+  }
+  ene = warp_sum(ene);
+  ens = warp_sum(ens);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&hist[nb], ene);
+    atomicAdd(&hist[nb + 1], ens);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x)
+    if (hist[i] != 0.0) atomicAdd(&out[i], hist[i]);
+}
+
+// fixed-point accumulation exactly as spectrum.wgsl:19-39 (u32, truncating)
+__global__ void k_diag_fixed(const float2* __restrict__ w, uint32_t* bins, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const int nb = n / 2 + 1;
+  const float kcut = (float)(n / 3.0);
+  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
+  const float k2 = kx * kx + ky * ky;
+  if (k2 == 0.f || !(fabsf(kx) < kcut && fabsf(ky) < kcut)) return;
+  const float2 a = w[idx];
+  const float n2 = (float)n * (float)n;
+  const float ens = 0.5f * (a.x * a.x + a.y * a.y) / (n2 * n2);
+  const float ene = ens / k2;
+  const uint32_t b = min((uint32_t)(sqrtf(k2) + 0.5f), (uint32_t)(nb - 1));
+  atomicAdd(&bins[b], (uint32_t)(ene * 1e8f));
+  atomicAdd(&bins[nb], (uint32_t)(ene * 1e6f));
+  atomicAdd(&bins[nb + 1], (uint32_t)(ens * 1e6f));
+}
+
+// zonal mean of u per row (spectrum.wgsl:41-68), accumulated in FP64
+__global__ void k_zonal_mean(const float2* __restrict__ vel, float* zonal, int n) {
+  const int row = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += (double)vel[(size_t)row * n + i].x;
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < (int)blockDim.x / 32; ++i) s += red[i];
+    zonal[row] = (float)(s / n);
+  }
+}
+
+// ------------------------------------------------------------------ dye
+// JS toHalf (solver.js:20-41): f32 -> binary16 by mantissa truncation
+__device__ __forceinline__ uint16_t to_half_trunc(float value) {
+  const uint32_t x = __float_as_uint(value);
+  const uint32_t sign = (x >> 16) & 0x8000u;
+  int exp = (int)((x >> 23) & 0xffu);
+  uint32_t mant = x & 0x7fffffu;
+  if (exp == 255) return (uint16_t)(sign | 0x7c00u | (mant ? 0x200u : 0u));
+  exp = exp - 127 + 15;
+  if (exp >= 31) return (uint16_t)(sign | 0x7c00u);
+  if (exp <= 0) {
+    if (exp < -10) return (uint16_t)sign;
+    mant = (mant | 0x800000u) >> (1 - exp);
+    return (uint16_t)(sign | (mant >> 13));
+  }
+  return (uint16_t)(sign | ((uint32_t)exp << 10) | (mant >> 13));
+}
+
+// 'bands' pattern (solver.js:450-466), computed in double like the JS
+__global__ void k_paint_bands(ushort4* dye, int m) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= m * m) return;
+  const int row = idx / m, col = idx % m;
+  const double fy = (double)row / m, fx = (double)col / m;
+  const double band = 0.5 + 0.5 * tanh(6.0 * sin(fy * 3.14159265358979323846 * 12.0));
+  const double mix = 0.5 + 0.5 * sin(fx * 3.14159265358979323846 * 2.0);
+  const double warm[3] = {1.0, 0.45, 0.22}, cool[3] = {0.28, 0.62, 1.0};
+  uint16_t c[3];
+  for (int k = 0; k < 3; ++k) c[k] = to_half_trunc((float)(band * (warm[k] * mix + cool[k] * (1.0 - mix)) * 0.9));
+  dye[idx] = make_ushort4(c[0], c[1], c[2], to_half_trunc(1.0f));
+}
+
+struct Rgba {
+  float r, g, b, a;
+};
+__device__ __forceinline__ Rgba load_texel(const ushort4* __restrict__ t, int x, int y, int m) {
+  const ushort4 u = __ldg(t + (size_t)y * m + x);
+  return {__half2float(__ushort_as_half(u.x)), __half2float(__ushort_as_half(u.y)),
+          __half2float(__ushort_as_half(u.z)), __half2float(__ushort_as_half(u.w))};
+}
+__device__ __forceinline__ int wrapi(int i, int m) { return ((i % m) + m) % m; }
+
+// bilinear velocity at normalised p (dye.wgsl:20-38)
+__device__ __forceinline__ float2 sample_vel(const float2* __restrict__ vel, float px, float py, int n) {
+  const float nf = (float)n;
+  const float gx = px * nf - 0.5f, gy = py * nf - 0.5f;
+  const float bx = floorf(gx), by = floorf(gy);
+  const float fx = gx - bx, fy = gy - by;
+  const int ix = (int)bx, iy = (int)by;
+  const int x0 = wrapi(ix, n), x1 = wrapi(ix + 1, n), y0 = wrapi(iy, n), y1 = wrapi(iy + 1, n);
+  const float2 v00 = __ldg(vel + (size_t)y0 * n + x0), v10 = __ldg(vel + (size_t)y0 * n + x1);
+  const float2 v01 = __ldg(vel + (size_t)y1 * n + x0), v11 = __ldg(vel + (size_t)y1 * n + x1);
+  const float ax = v00.x * (1.f - fx) + v10.x * fx, ay = v00.y * (1.f - fx) + v10.y * fx;
+  const float bx2 = v01.x * (1.f - fx) + v11.x * fx, by2 = v01.y * (1.f - fx) + v11.y * fx;
+  return make_float2(ax * (1.f - fy) + bx2 * fy, ay * (1.f - fy) + by2 * fy);
+}
+
+// midpoint back-trace (dye.wgsl:40-45)
+__device__ __forceinline__ float2 trace_pos(const float2* __restrict__ vel, float px, float py, float h, int n) {
+  const float2 v1 = sample_vel(vel, px, py, n);
+  float mx = px - 0.5f * (v1.x * h) + 1.f, my = py - 0.5f * (v1.y * h) + 1.f;
+  mx -= floorf(mx);
+  my -= floorf(my);
+  const float2 v2 = sample_vel(vel, mx, my, n);
+  float sx = px - v2.x * h + 1.f, sy = py - v2.y * h + 1.f;
+  return make_float2(sx - floorf(sx), sy - floorf(sy));
+}
+
+// software form of a linear-filtered, repeat-addressed texture sample
+__device__ __forceinline__ Rgba sample_dye(const ushort4* __restrict__ tex, float sx, float sy, int m,
+                                           Rgba* lo = nullptr, Rgba* hi = nullptr) {
+  const float mf = (float)m;
+  const float gx = sx * mf - 0.5f, gy = sy * mf - 0.5f;
+  const float bx = floorf(gx), by = floorf(gy);
+  const float fx = gx - bx, fy = gy - by;
+  const int x0 = wrapi((int)bx, m), x1 = wrapi((int)bx + 1, m);
+  const int y0 = wrapi((int)by, m), y1 = wrapi((int)by + 1, m);
+  const Rgba c00 = load_texel(tex, x0, y0, m), c10 = load_texel(tex, x1, y0, m);
+  const Rgba c01 = load_texel(tex, x0, y1, m), c11 = load_texel(tex, x1, y1, m);
+  auto lerp2 = [&](float a00, float a10, float a01, float a11) {
+    const float a = a00 * (1.f - fx) + a10 * fx, b = a01 * (1.f - fx) + a11 * fx;
+    return a * (1.f - fy) + b * fy;
+  };
+  if (lo) {
+    lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
+    lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
+    lo->b = fminf(fminf(c00.b, c10.b), fminf(c01.b, c11.b));
+    hi->r = fmaxf(fmaxf(c00.r, c10.r), fmaxf(c01.r, c11.r));
+    hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
+    hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
+  }
+  return {lerp2(c00.r, c10.r, c01.r, c11.r), lerp2(c00.g, c10.g, c01.g, c11.g),
+          lerp2(c00.b, c10.b, c01.b, c11.b), lerp2(c00.a, c10.a, c01.a, c11.a)};
+}
+
+__device__ __forceinline__ ushort4 pack_rgba(float r, float g, float b, float a) {
+  return make_ushort4(__half_as_ushort(__float2half_rn(r)), __half_as_ushort(__float2half_rn(g)),
+                      __half_as_ushort(__float2half_rn(b)), __half_as_ushort(__float2half_rn(a)));
+}
+
+// advect_fwd / advect_back (dye.wgsl:58-74): dst = src sampled at trace(p, sign*dt/2pi)
+__global__ void k_dye_advect(const float2* __restrict__ vel, const ushort4* __restrict__ src, ushort4* dst,
+                             const float* __restrict__ dtbuf, float sign, int n, int m) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= m || gy >= m) return;
+  const float mf = (float)m;
+  const float px = ((float)gx + 0.5f) / mf, py = ((float)gy + 0.5f) / mf;
+  const float h = sign * dtbuf[0] / kTwoPiF;
+  const float2 s = trace_pos(vel, px, py, h, n);
+  const Rgba c = sample_dye(src, s.x, s.y, m);
+  dst[(size_t)gy * m + gx] = pack_rgba(c.r, c.g, c.b, c.a);
+}
+
+// advect_corr (dye.wgsl:76-113): BFECC correction, MacCormack clamp, fade, splat dye
+__global__ void k_dye_correct(const float2* __restrict__ vel, const ushort4* __restrict__ src,
+                              const ushort4* __restrict__ aux, ushort4* dst, const float* __restrict__ dtbuf,
+                              const DevParams* __restrict__ params, const DevSplats* __restrict__ S, int n,
+                              int m) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= m || gy >= m) return;
+  const float mf = (float)m;
+  const float px = ((float)gx + 0.5f) / mf, py = ((float)gy + 0.5f) / mf;
+  const float h = dtbuf[0] / kTwoPiF;
+  const float2 s = trace_pos(vel, px, py, h, n);
+  Rgba lo, hi;
+  const Rgba a = sample_dye(src, s.x, s.y, m, &lo, &hi);
+  const Rgba b = sample_dye(aux, s.x, s.y, m);
+  const float fade = params->dye_fade;
+  float r = fminf(fmaxf(1.5f * a.r - 0.5f * b.r, lo.r), hi.r) * fade;
+  float g = fminf(fmaxf(1.5f * a.g - 0.5f * b.g, lo.g), hi.g) * fade;
+  float bb = fminf(fmaxf(1.5f * a.b - 0.5f * b.b, lo.b), hi.b) * fade;
+  const int cnt = S->count;
+  for (int i = 0; i < cnt; ++i) {
+    const DevSplat sp = S->items[i];
+    const float rx = sepf(px, sp.x), ry = sepf(py, sp.y);
+    const float sig2 = fmaxf(sp.radius * sp.radius, 1e-8f);
+    const float r2 = rx * rx + ry * ry;
+    if (r2 < 9.f * sig2) {
+      const float wgt = sp.dye_amp * expf(-r2 / sig2);
+      r += sp.r * wgt;
+      g += sp.g * wgt;
+      bb += sp.b * wgt;
+    }
+  }
+  dst[(size_t)gy * m + gx] = pack_rgba(r, g, bb, 1.f);
+}
+
+}  // namespace s2d

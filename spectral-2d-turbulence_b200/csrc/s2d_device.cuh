@@ -1,0 +1,139 @@
+// s2d_device.cuh -- device-side parameter blocks and per-cell helpers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "fft_core.cuh"
+
+namespace s2d {
+
+constexpr float kTwoPiF = 6.28318530717958647f;  // TWO_PI, common.wgsl:5
+
+// Params uniform of the reference (common.wgsl:8-21), plus the grid constants
+// the reference templates into each shader (shaders.js:20-28).  Lives in
+// device memory; written by configure(), read by every stage kernel.
+struct DevParams {
+  float beta, mu, nu_h;
+  int32_t hyper_p;
+  float force_amp, force_k, force_width;
+  uint32_t step_index;
+  float dx, cfl, dt_min, dt_max;
+  float dye_fade, kcut, force_norm;
+  int32_t n;
+};
+
+// Splat / Splats uniform (common.wgsl:23-40)
+struct DevSplat {
+  float x, y, vx, vy;
+  float r, g, b, radius;
+  float amp, dye_amp, pad0, pad1;
+};
+struct DevSplats {
+  int32_t count, pad0, pad1, pad2;
+  DevSplat items[8];
+};
+
+// RK3 coefficient rows [cA, a, cB, b] (solver.js:11-15)
+__host__ __device__ constexpr float rk_cA(int s) { return s == 0 ? 0.f : s == 1 ? 0.75f : 1.f / 3.f; }
+__host__ __device__ constexpr float rk_cB(int s) { return s == 0 ? 1.f : s == 1 ? 0.25f : 2.f / 3.f; }
+__host__ __device__ constexpr float rk_a(int s) { return s == 0 ? 0.f : s == 1 ? 0.5f : 1.f; }
+__host__ __device__ constexpr float rk_b(int s) { return s == 0 ? 1.f : s == 1 ? -0.5f : 0.5f; }
+
+// signed wavenumber of FFT index i (common.wgsl:50-55)
+template <int N> __device__ __forceinline__ float wn(int i) { return (float)(i < N / 2 ? i : i - N); }
+__device__ __forceinline__ float wn_rt(int i, int n) { return (float)(i < n / 2 ? i : i - n); }
+
+// PCG-style hash (common.wgsl:76-80) and its unit float (common.wgsl:82-84)
+__host__ __device__ __forceinline__ uint32_t hash1(uint32_t x) {
+  uint32_t v = x * 747796405u + 2891336453u;
+  v = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+  return (v >> 22u) ^ v;
+}
+__device__ __forceinline__ float hashf(uint32_t a, uint32_t b) {
+  return __uint2float_rn(hash1(a ^ hash1(b))) * 2.3283064365386963e-10f;
+}
+
+// k^(2p) as (k2)^p for integer p >= 0
+__device__ __forceinline__ float powi(float k2, int p) {
+  float r = 1.f;
+  for (int i = 0; i < p; ++i) r *= k2;
+  return r;
+}
+
+// White-in-time stochastic forcing of one spectral cell (solver.wgsl:77-92).
+// Caller guarantees the cell is in the dealias band with k2 > 0.
+__device__ __forceinline__ float2 stochastic_term(const DevParams& P, int n, int row, int col, float kx,
+                                                  float ky, float k2, float dt) {
+  const float d = (sqrtf(k2) - P.force_k) / P.force_width;
+  const float env = expf(-(d * d));
+  if (!(env > 1e-4f)) return make_float2(0.f, 0.f);
+  const bool canon = ky > 0.f || (ky == 0.f && kx > 0.f);
+  const uint32_t hr = canon ? (uint32_t)row : (uint32_t)((n - row) & (n - 1));
+  const uint32_t hc = canon ? (uint32_t)col : (uint32_t)((n - col) & (n - 1));
+  const float sgn = canon ? 1.f : -1.f;
+  const float ph = kTwoPiF * hashf(hr * (uint32_t)n + hc, P.step_index);
+  const float amp = P.force_amp * env * P.force_norm / sqrtf(fmaxf(dt, 1e-6f));
+  float s, c;
+  sincosf(ph, &s, &c);
+  return make_float2(amp * c, sgn * amp * s);
+}
+
+// Integrating factor over half a step: E(dt/2) = exp(L dt/2),
+// L = -mu - nu_h k2^p + i beta kx/k2 (solver.wgsl:97-101, spectral2d.py:26)
+struct HalfFactor {
+  float mag;   // exp(Re L * dt/2)
+  float2 rot;  // exp(i Im L * dt/2)
+};
+__device__ __forceinline__ HalfFactor half_factor(const DevParams& P, float kx, float k2, float dt) {
+  HalfFactor h;
+  const float re = -P.mu - P.nu_h * powi(k2, P.hyper_p);
+  h.mag = expf(re * (0.5f * dt));
+  if (P.beta != 0.f) {
+    const float im = P.beta * kx / k2;
+    float s, c;
+    sincosf(im * (0.5f * dt), &s, &c);
+    h.rot = make_float2(c, s);
+  } else {
+    h.rot = make_float2(1.f, 0.f);
+  }
+  return h;
+}
+
+// wout = cA E(a dt) w0 + cB E(b dt) (wcur + dt rhs) for stage s, using
+// E(dt) = E(dt/2)^2 and E(-dt/2) = 1/E(dt/2) (one exp and one sincos per cell).
+template <int S>
+__device__ __forceinline__ float2 rk_update(const HalfFactor& h, float2 w0, float2 wcur, float2 rhs, float dt) {
+  const float2 adv = make_float2(wcur.x + dt * rhs.x, wcur.y + dt * rhs.y);
+  const float2 e_half = cscale(h.rot, h.mag);
+  if constexpr (S == 0) {
+    const float2 e_full = cscale(cmul(h.rot, h.rot), h.mag * h.mag);
+    return cmul(e_full, adv);
+  } else if constexpr (S == 1) {
+    const float2 e_mhalf = cscale(cconj(h.rot), 1.f / h.mag);
+    const float2 a = cmul(e_half, w0), b = cmul(e_mhalf, adv);
+    return make_float2(0.75f * a.x + 0.25f * b.x, 0.75f * a.y + 0.25f * b.y);
+  } else {
+    const float2 e_full = cscale(cmul(h.rot, h.rot), h.mag * h.mag);
+    const float2 a = cmul(e_full, w0), b = cmul(e_half, adv);
+    return make_float2((1.f / 3.f) * a.x + (2.f / 3.f) * b.x, (1.f / 3.f) * a.y + (2.f / 3.f) * b.y);
+  }
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// CFL dt from the maximum of |u|+|v| (reduce.wgsl:54-62)
+__device__ __forceinline__ float cfl_dt(const DevParams& P, float speed) {
+  float dt = P.dt_max;
+  if (speed > 1e-8f) dt = fminf(P.dt_max, P.cfl * P.dx / speed);
+  return fmaxf(dt, P.dt_min);
+}
+
+}  // namespace s2d

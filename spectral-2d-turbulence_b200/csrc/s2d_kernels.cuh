@@ -1,0 +1,390 @@
+// s2d_kernels.cuh -- sm_100a kernels of the integrating-factor RK3 step.
+//
+// Fused step (one RK stage = two kernels, both whole-line FFTs in shared memory):
+//
+//   k_phys_cols  "physical columns": for a tile of GA columns x, read the
+//                x-transformed packs PA(ky,x) = FFT_x^-1(w + i u_hat),
+//                PB(ky,x) = FFT_x^-1(v_hat), y-IFFT both to (omega, u, v)(y,x),
+//                form u*omega + i v*omega, y-FFT it and store the dealiased rows
+//                Z(ky,x) (|ky| < N/3 only).  At the last stage it also writes the
+//                velocity (u,v) for the dye and reduces max|u|+|v| for the CFL dt.
+//   k_spec_rows  "spectral row pairs": for the rows ky and -ky, x-FFT Z, unpack the
+//                two real spectra through the partner row (Hermitian unpack),
+//                form N_hat = i kx q1 + i ky q2 with the 2/3 mask, add pointer and
+//                stochastic forcing, apply the integrating-factor RK3 stage update,
+//                then pack the NEXT stage's (w + i u_hat, v_hat), scale 1/N^2 and
+//                x-IFFT them into PA, PB.
+//
+// Per stage this moves ~45 N^2 bytes in k_spec_rows and ~21 N^2 in k_phys_cols
+// instead of the reference's 7 full passes.  The standalone kernels at the end
+// (velocity_pack, nl_pack, assemble, rk3, fft rows/cols) reproduce the
+// reference's unfused stages one for one, for the per-stage test hooks.
+#pragma once
+#include "s2d_device.cuh"
+
+namespace s2d {
+
+template <int N_> struct Tune {
+  static constexpr int N = N_;
+  static constexpr int V = 16;
+  static constexpr int T = N / V;
+  using PL = LinePlan<N, V>;
+  // physical-column kernel: GA columns per CTA, lanes run over columns first
+  static constexpr int GA = N >= 4096 ? 2 : ((256 / T) > 4 ? ((256 / T) < N ? (256 / T) : N) : 4);
+  static constexpr int A_THREADS = GA * T;
+  static constexpr int A_LDS = PL::stride(GA >= 16 ? 1 : 16 / GA);
+  static constexpr int A_GRID = N / GA;
+  // spectral-row kernel: PPB row pairs (2*PPB rows) per CTA, lanes run along a row
+  static constexpr int PPB = T >= 64 ? 1 : ((64 / T) < N / 2 ? (64 / T) : N / 2);
+  static constexpr int B_ROWS = 2 * PPB;
+  static constexpr int B_THREADS = B_ROWS * T;
+  static constexpr int B_LDS = PL::stride(T >= 16 ? 0 : T);
+  static constexpr int B_GRID = (N / 2) / PPB;
+  static constexpr float KCUT = (float)(N / 3.0);
+  static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
+  static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
+  static constexpr size_t COLS_SMEM = sizeof(float2) * GA * A_LDS;
+  static constexpr size_t ROWS_SMEM = sizeof(float2) * B_ROWS * B_LDS;
+};
+
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// ---------------------------------------------------------------------------------------
+// arguments of the fused kernels
+struct PhysArgs {
+  const float2* pa;     // x-transformed packs, [ky][x]
+  const float2* pb;
+  float2* z;            // product spectrum after the y-FFT, [ky][x], in-band rows
+  float2* vel;          // physical (u, v), [y][x]
+  float* partials;      // per-CTA max |u|+|v|
+  unsigned* ticket;     // last-CTA-done counter
+  float* dt_out;        // dt slot written by the last CTA: [dt, speed]
+  const DevParams* params;
+  const float2* tw;
+  int reduce;           // finalize the CFL dt into dt_out
+};
+
+struct SpecArgs {
+  const float2* z;      // product spectrum (ky, x), in-band rows
+  const float2* w0;     // state at the start of the step
+  const float2* wcur;   // state entering this stage (prime: the state to pack)
+  float2* wout;         // state leaving this stage
+  const float2* fptr;   // pointer-force spectrum, or nullptr
+  float2* pa;           // next-stage packs, x-transformed, [ky][x]
+  float2* pb;
+  const float* dt;      // current dt slot
+  const DevParams* params;
+  const float2* tw;
+  int stochastic;       // force_amp > 0
+};
+
+// ---------------------------------------------------------------------------------------
+// physical columns: MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage
+// (stage + velocity + speed)
+// one tile of GA columns; returns this thread's max |u|+|v| (MODE != 1)
+template <int N, int MODE>
+__device__ __forceinline__ float phys_cols_tile(const PhysArgs& a, int tile, float2* smem) {
+  using TU = Tune<N>;
+  constexpr int V = TU::V, T = TU::T, GA = TU::GA, LDS = TU::A_LDS;
+  const int tid = threadIdx.x;
+  const int g = tid % GA, t = tid / GA;
+  const int x = tile * GA + g;
+  float2* const bufs[2] = {smem + g * LDS, smem + (GA + g) * LDS};
+
+  float2 v[2][V];
+#pragma unroll
+  for (int m = 0; m < V; ++m) {
+    const size_t o = (size_t)(t + T * m) * N + x;
+    v[0][m] = __ldcs(a.pa + o);
+    v[1][m] = __ldcs(a.pb + o);
+  }
+  fft_lines<N, V, +1, 2>(v, bufs, t, a.tw, CtaSync{});
+  // v[0][m] = (omega, u), v[1][m].x = v at physical row y = t + T*m
+
+  float speed = 0.f;
+  if constexpr (MODE != 1) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const float u = v[0][m].y, w = v[1][m].x;
+      a.vel[(size_t)(t + T * m) * N + x] = make_float2(u, w);
+      speed = fmaxf(speed, fabsf(u) + fabsf(w));
+    }
+  }
+  if constexpr (MODE != 0) {
+    float2 z[1][V];
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const float om = v[0][m].x;
+      z[0][m] = make_float2(v[0][m].y * om, v[1][m].x * om);
+    }
+    float2* const zb[1] = {bufs[0]};
+    fft_lines<N, V, -1, 1>(z, zb, t, a.tw, CtaSync{});
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const int row = t + T * m;
+      if (fabsf(wn<N>(row)) < TU::KCUT) a.z[(size_t)row * N + x] = z[0][m];
+    }
+  }
+  return speed;
+}
+
+template <int N, int MODE>
+__global__ void __launch_bounds__(Tune<N>::A_THREADS) k_phys_cols(PhysArgs a) {
+  using TU = Tune<N>;
+  extern __shared__ float2 smem[];
+  float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
+  const int tid = threadIdx.x;
+  if constexpr (MODE != 1) {
+    __shared__ float red[32];
+    __shared__ int last;
+    speed = warp_max(speed);
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0) red[warp] = speed;
+    __syncthreads();
+    if (warp == 0) {
+      float s = lane < (TU::A_THREADS + 31) / 32 ? red[lane] : 0.f;
+      s = warp_max(s);
+      if (lane == 0) {
+        a.partials[blockIdx.x] = s;
+        int is_last = 0;
+        if (a.reduce) {
+          __threadfence();
+          const unsigned k = atomicAdd(a.ticket, 1u);
+          is_last = (k == gridDim.x - 1);
+        }
+        last = is_last;
+      }
+    }
+    __syncthreads();
+    if (last) {
+      float s = 0.f;
+      for (int i = tid; i < (int)gridDim.x; i += blockDim.x) s = fmaxf(s, __ldcg(a.partials + i));
+      s = warp_max(s);
+      if (lane == 0) red[warp] = s;
+      __syncthreads();
+      if (tid == 0) {
+        float m = 0.f;
+        for (int i = 0; i < (TU::A_THREADS + 31) / 32; ++i) m = fmaxf(m, red[i]);
+        a.dt_out[0] = cfl_dt(*a.params, m);
+        a.dt_out[1] = m;
+        *a.ticket = 0u;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// spectral row pairs: MODE -1 = prime (pack wcur only), 0/1/2 = RK stage
+template <int N, int MODE, bool PTR>
+__device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, float2* smem) {
+  using TU = Tune<N>;
+  constexpr int V = TU::V, T = TU::T, LDS = TU::B_LDS;
+  constexpr float KCUT = TU::KCUT;
+  const int tid = threadIdx.x;
+  const int t = tid % T, slot = tid / T;
+  const int pair = tile * TU::PPB + (slot >> 1);
+  const int which = slot & 1;
+  const int row = pair == 0 ? (which ? N / 2 : 0) : (which ? N - pair : pair);
+  const int pslot = pair == 0 ? slot : (slot ^ 1);
+  float2* const own0 = smem + (2 * slot) * LDS;
+  float2* const own1 = smem + (2 * slot + 1) * LDS;
+  const float ky = wn<N>(row);
+  const bool row_band = fabsf(ky) < KCUT;
+  const size_t rbase = (size_t)row * N;
+
+  float2 nh[V];
+  if constexpr (MODE >= 0) {
+    // the first pair of this CTA has the smallest |ky|: the CTA is uniformly in/out of band work
+    const bool cta_band = (float)(tile * TU::PPB) < KCUT;
+    if (cta_band) {
+      float2 zz[1][V];
+#pragma unroll
+      for (int m = 0; m < V; ++m) zz[0][m] = row_band ? __ldcs(a.z + rbase + t + T * m) : make_float2(0.f, 0.f);
+      float2* const zb[1] = {own0};
+      fft_lines<N, V, -1, 1>(zz, zb, t, a.tw, CtaSync{});
+#pragma unroll
+      for (int m = 0; m < V; ++m) own0[LinePlan<N, V>::pad(t + T * m)] = zz[0][m];
+      __syncthreads();
+      const float2* pbuf = smem + (2 * pslot) * LDS;
+#pragma unroll
+      for (int m = 0; m < V; ++m) {
+        const int c = t + T * m;
+        const float kx = wn<N>(c);
+        const float2 zk = zz[0][m];
+        const float2 zm = cconj(pbuf[LinePlan<N, V>::pad((N - c) & (N - 1))]);
+        // q1 = (Z_k + conj Z_-k)/2, q2 = -i (Z_k - conj Z_-k)/2 (solver.wgsl:68-72)
+        const float2 q1 = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+        const float2 dd = csub(zk, zm);
+        const float2 q2 = make_float2(0.5f * dd.y, -0.5f * dd.x);
+        const bool band = row_band && fabsf(kx) < KCUT;
+        // N_hat = kx * (i q1) + ky * (i q2)
+        nh[m] = band ? make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x) : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int m = 0; m < V; ++m) nh[m] = make_float2(0.f, 0.f);
+    }
+  }
+
+  float2 p[2][V];
+  {
+    const DevParams& P = *a.params;
+    float dt = 0.f;
+    if constexpr (MODE >= 0) dt = __ldg(a.dt);
+    constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const int c = t + T * m;
+      const size_t o = rbase + c;
+      const float kx = wn<N>(c);
+      const float k2 = kx * kx + ky * ky;
+      float2 w;
+      if constexpr (MODE < 0) {
+        w = a.wcur[o];
+      } else {
+        const float2 wc = a.wcur[o];
+        const float2 w0 = MODE == 0 ? wc : a.w0[o];
+        const bool band = row_band && fabsf(kx) < KCUT;
+        float2 rhs = make_float2(-nh[m].x, -nh[m].y);
+        if constexpr (PTR) {
+          if (band) rhs = cadd(rhs, __ldg(a.fptr + o));
+        }
+        if (a.stochastic && band && k2 > 0.f) rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
+        if (k2 == 0.f) {
+          w = make_float2(0.f, 0.f);
+        } else {
+          const HalfFactor hf = half_factor(P, kx, k2, dt);
+          w = rk_update<MODE>(hf, w0, wc, rhs, dt);
+        }
+        a.wout[o] = w;
+      }
+      // next-stage packs, scaled by the 1/N^2 of the inverse 2D transform
+      const float inv = k2 > 0.f ? 1.f / k2 : 0.f;
+      const float fa = (1.f - ky * inv) * inv_n2;     // w + i u_hat = w (1 - ky/k2)
+      const float fb = kx * inv * inv_n2;              // v_hat = -i kx w / k2
+      p[0][m] = make_float2(w.x * fa, w.y * fa);
+      p[1][m] = make_float2(w.y * fb, -w.x * fb);
+    }
+  }
+  float2* const pbufs[2] = {own0, own1};
+  fft_lines<N, V, +1, 2>(p, pbufs, t, a.tw, CtaSync{});
+#pragma unroll
+  for (int m = 0; m < V; ++m) {
+    const size_t o = rbase + t + T * m;
+    a.pa[o] = p[0][m];
+    a.pb[o] = p[1][m];
+  }
+}
+
+template <int N, int MODE, bool PTR>
+__global__ void __launch_bounds__(Tune<N>::B_THREADS) k_spec_rows(SpecArgs a) {
+  extern __shared__ float2 smem[];
+  spec_rows_tile<N, MODE, PTR>(a, blockIdx.x, smem);
+}
+
+// ---------------------------------------------------------------------------------------
+// standalone 2D FFT passes (Fft2D.run, fft.js:81-92): rows (x) then columns (y).
+// SIGN -1 forward unscaled; +1 inverse scaled 1/N per pass (fft.js:58-59).
+template <int N, int SIGN>
+__global__ void __launch_bounds__(Tune<N>::B_THREADS) k_fft_rows(float2* data, const float2* tw) {
+  using TU = Tune<N>;
+  constexpr int V = TU::V, T = TU::T;
+  extern __shared__ float2 smem[];
+  const int t = threadIdx.x % T, slot = threadIdx.x / T;
+  const size_t base = (size_t)(blockIdx.x * TU::B_ROWS + slot) * N;
+  float2 x[1][V];
+#pragma unroll
+  for (int m = 0; m < V; ++m) x[0][m] = data[base + t + T * m];
+  float2* const b[1] = {smem + slot * TU::B_LDS};
+  fft_lines<N, V, SIGN, 1>(x, b, t, tw, CtaSync{});
+  constexpr float sc = SIGN > 0 ? 1.0f / N : 1.0f;
+#pragma unroll
+  for (int m = 0; m < V; ++m) data[base + t + T * m] = cscale(x[0][m], sc);
+}
+
+template <int N, int SIGN>
+__global__ void __launch_bounds__(Tune<N>::A_THREADS) k_fft_cols(float2* data, const float2* tw) {
+  using TU = Tune<N>;
+  constexpr int V = TU::V, T = TU::T, GA = TU::GA;
+  extern __shared__ float2 smem[];
+  const int g = threadIdx.x % GA, t = threadIdx.x / GA;
+  const int col = blockIdx.x * GA + g;
+  float2 x[1][V];
+#pragma unroll
+  for (int m = 0; m < V; ++m) x[0][m] = data[(size_t)(t + T * m) * N + col];
+  float2* const b[1] = {smem + g * TU::A_LDS};
+  fft_lines<N, V, SIGN, 1>(x, b, t, tw, CtaSync{});
+  constexpr float sc = SIGN > 0 ? 1.0f / N : 1.0f;
+#pragma unroll
+  for (int m = 0; m < V; ++m) data[(size_t)(t + T * m) * N + col] = cscale(x[0][m], sc);
+}
+
+// ---------------------------------------------------------------------------------------
+// elementwise reference stages (one thread per cell, any N)
+static __global__ void k_velocity_pack(const float2* __restrict__ w, float2* pa, float2* pb, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
+  const float k2 = kx * kx + ky * ky;
+  const float inv = k2 > 0.f ? 1.f / k2 : 0.f;
+  const float2 ww = w[idx];
+  const float2 iw = make_float2(-ww.y, ww.x);
+  const float2 uh = cscale(iw, ky * inv);
+  const float2 vh = cscale(iw, -kx * inv);
+  pa[idx] = make_float2(ww.x - uh.y, ww.y + uh.x);   // w + i*uh (solver.wgsl:38)
+  pb[idx] = vh;
+}
+
+static __global__ void k_nl_pack(const float2* __restrict__ pa, const float2* __restrict__ pb, float2* physz,
+                          float2* vel, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float2 a = pa[idx];
+  const float om = a.x, u = a.y, v = pb[idx].x;
+  physz[idx] = make_float2(u * om, v * om);
+  vel[idx] = make_float2(u, v);
+}
+
+static __global__ void k_assemble(const float2* __restrict__ physz, const float2* __restrict__ fhat,
+                           const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
+                           float2* rhs, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const DevParams& P = *params;
+  const int col = idx & (n - 1), row = idx / n;
+  const float kx = wn_rt(col, n), ky = wn_rt(row, n);
+  const float k2 = kx * kx + ky * ky;
+  const float2 zk = physz[idx];
+  const float2 zm = cconj(physz[((n - row) & (n - 1)) * n + ((n - col) & (n - 1))]);
+  const float2 q1 = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+  const float2 dd = csub(zk, zm);
+  const float2 q2 = make_float2(0.5f * dd.y, -0.5f * dd.x);
+  const float2 nhat = make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x);
+  const float mask = (fabsf(kx) < P.kcut && fabsf(ky) < P.kcut) ? 1.f : 0.f;
+  float2 f = cscale(csub(fhat[idx], nhat), mask);
+  if (P.force_amp > 0.f && mask > 0.f && k2 > 0.f)
+    f = cadd(f, stochastic_term(P, n, row, col, kx, ky, k2, dtbuf[0]));
+  rhs[idx] = f;
+}
+
+template <int S>
+__global__ void k_rk3(const float2* __restrict__ w0, const float2* __restrict__ wcur, float2* wout,
+                      const float2* __restrict__ rhs, const float* __restrict__ dtbuf,
+                      const DevParams* __restrict__ params, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
+  const float k2 = kx * kx + ky * ky;
+  if (k2 == 0.f) {
+    wout[idx] = make_float2(0.f, 0.f);
+    return;
+  }
+  const float dt = dtbuf[0];
+  const HalfFactor hf = half_factor(*params, kx, k2, dt);
+  wout[idx] = rk_update<S>(hf, w0[idx], wcur[idx], rhs[idx], dt);
+}
+
+}  // namespace s2d

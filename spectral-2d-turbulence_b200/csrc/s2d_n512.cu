@@ -1,0 +1,10 @@
+// Kernel instantiations for N = 512 (one translation unit per grid size so the
+// per-size template expansions compile in parallel).
+#include "s2d_ops.cuh"
+
+namespace s2d {
+const NOps* ops_n512() {
+  static const NOps o = OpsImpl<512>::make();
+  return &o;
+}
+}  // namespace s2d

@@ -1,0 +1,135 @@
+"""Diagnostics (FP64 and the reference's fixed point) and dye advection."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_helpers import config, current_state, set_fixed_dt
+from oracle import wgsl_oracle as wo
+from oracle.spectral_oracle import SpectralOracle, random_field
+
+pytestmark = pytest.mark.gpu
+
+
+def test_read_before_copy_is_null(pkg):
+    s = pkg.Solver.create(n=64, dyeScale=1)
+    try:
+        assert s.readDiagnostics() is None                                  # solver.js:571-573
+        s.encodeDiagnostics()
+        s.copyDiagnostics()
+        assert s.readDiagnostics() is not None
+        assert s.readDiagnostics() is None                                  # read state back to idle
+    finally:
+        s.destroy()
+
+
+@pytest.mark.parametrize("n", [64, 512])
+def test_fp64_diagnostics(pkg, n):
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
+        s.seedPhysical(random_field(n, k0=n / 10, seed=7, amplitude=5.0))
+        s.encodePrime()
+        w = current_state(s)
+        s.encodeDiagnostics()
+        s.copyDiagnostics()
+        d = s.readDiagnostics()
+        ref = SpectralOracle(n=n)
+        ref.w = w.astype(np.complex128)
+        assert abs(d["energy"] / ref.energy() - 1) <= 1e-12
+        assert abs(d["enstrophy"] / ref.enstrophy() - 1) <= 1e-12
+        assert np.allclose(d["spectrum"], ref.spectrum()[1], rtol=1e-11, atol=1e-300)
+        # zonal mean of u of the last velocity evaluation (here: the prime's, from w)
+        zonal_ref = ref.zonal_mean_u()
+        assert np.max(np.abs(d["zonal"] - zonal_ref)) <= 1e-5 * np.max(np.abs(ref.velocity()[0]))
+        dt, speed = s.getBuffer("dt")[:2]
+        assert d["dt"] == dt and d["maxSpeed"] == speed
+    finally:
+        s.destroy()
+
+
+def test_zonal_mean_is_the_stage2_velocity(pkg):
+    n, dt = 128, 2e-3
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(beta=10.0, viscosity=1.0))
+        s.seedPhysical(random_field(n, k0=12, seed=8, amplitude=6.0))
+        w0 = current_state(s)
+        set_fixed_dt(s, dt)
+        s.encodeStep()
+        s.encodeDiagnostics(); s.copyDiagnostics()
+        d = s.readDiagnostics()
+        ref = SpectralOracle(n=n, beta=10.0, nu_h=float(s.paramsF[2]), hyper_p=4)
+        w = w0.astype(np.complex128)
+        e_full, e_half, e_mh = ref.factor(dt), ref.factor(dt / 2), ref.factor(-dt / 2)
+        w1 = e_full * (w + dt * ref.rhs(w))
+        w2 = 0.75 * e_half * w + 0.25 * e_mh * (w1 + dt * ref.rhs(w1))
+        ref.w = w2                          # the reference reads packA.y after stage 2 (solver.js:258)
+        want = ref.zonal_mean_u()
+        assert np.max(np.abs(d["zonal"] - want)) <= 2e-5 * np.max(np.abs(ref.velocity()[0]))
+    finally:
+        s.destroy()
+
+
+def test_fixed_point_diagnostics_match_restatement(pkg):
+    n = 128
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.seed(k0=14, amplitude=6, seed=3)
+        s.encodeDiagnostics(); s.copyDiagnostics()
+        s.readDiagnostics()
+        fx = s.readDiagnosticsFixed()
+        spec, e, z = wo.spectrum_fixed_point(s.getBuffer("state0"), n)
+        assert np.allclose(fx["spectrum"], spec, rtol=1e-5, atol=1e-7)
+        assert abs(fx["energy"] - e) <= 1e-5 * abs(e) + 1e-5
+        assert abs(fx["enstrophy"] - z) <= 1e-5 * abs(z) + 1e-5
+    finally:
+        s.destroy()
+
+
+# ---------------------------------------------------------------- dye
+@pytest.mark.parametrize("m_scale", [1, 2])
+def test_paint_bands(pkg, m_scale):
+    n = 64
+    s = pkg.Solver.create(n=n, dyeScale=m_scale)
+    try:
+        s.reset({"k0": 14, "amplitude": 6, "seed": 1, "dyePattern": "bands"})
+        got = s.currentDye
+        want = wo.paint_dye_bands(n * m_scale)
+        diff = np.abs(got.astype(np.int32) - want.astype(np.int32))
+        assert diff.max() <= 1 and np.mean(diff != 0) < 1e-3
+    finally:
+        s.destroy()
+
+
+def _splat_np(sp):
+    r = np.zeros(1, wo.SPLAT_DTYPE)[0]
+    r["x"], r["y"], r["dx"], r["dy"] = sp["x"], sp["y"], sp["dx"], sp["dy"]
+    r["r"], r["g"], r["b"] = sp["color"]
+    r["radius"], r["amp"], r["dye_amp"] = sp["radius"], sp["amp"], sp["dyeAmp"]
+    return r
+
+
+@pytest.mark.parametrize("m_scale", [1, 2])
+def test_dye_bfecc_step(pkg, m_scale):
+    n = 128
+    s = pkg.Solver.create(n=n, dyeScale=m_scale)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.02, dyeFade=0.999))
+        s.reset({"k0": 10, "amplitude": 8, "seed": 2, "dyePattern": "bands"})
+        splat = {"x": 0.4, "y": 0.7, "dx": 0.01, "dy": 0.0, "color": (1.0, 0.42, 0.28), "radius": 0.05,
+                 "amp": 0.0, "dyeAmp": 0.9}
+        s.setSplats([splat])
+        s.encodePrime()
+        dye0 = s.currentDye
+        vel = s.getBuffer("vel")
+        dt = float(s.getBuffer("dt")[0])
+        s.encodeDye()
+        got = wo.half_bits_to_f32(s.currentDye)
+        velf = np.stack([vel.real, vel.imag], axis=-1).astype(np.float32)
+        want = wo.half_bits_to_f32(wo.dye_step(dye0, velf, dt, 0.999, [_splat_np(splat)]))
+        diff = np.abs(got - want)
+        assert diff.max() <= 4e-3, diff.max()
+        assert diff.mean() <= 1e-5, diff.mean()
+        assert np.all(got[..., 3] == 1.0)
+    finally:
+        s.destroy()

@@ -1,0 +1,335 @@
+"""Parity of the CUDA path with the oracle: tables, FFTs, the fused RK3 step,
+forcing, CFL reduction, seeding, and the Taylor-Green invariants."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2, rel_linf
+from gpu_helpers import config, current_state, load_state, rate_for, set_fixed_dt
+from oracle import fft_oracle as fo
+from oracle import wgsl_oracle as wo
+from oracle.spectral_oracle import SpectralOracle, dealias_mask, random_field, wavenumbers
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [32, 64, 128, 256, 512, 1024, 2048, 4096]
+
+
+# ---------------------------------------------------------------- bit-exact tables
+@pytest.mark.parametrize("n", [2, 8, 32, 128, 512, 2048, 4, 16, 64, 256, 1024, 4096])
+def test_digit_reverse_bit_exact(pkg, fft_golden, n):
+    assert np.array_equal(pkg.digitReverseTable(n), fft_golden[f"rev_{n}"])
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_wavenumbers_and_mask_bit_exact(pkg, n):
+    wn = pkg.wavenumberTable(n)
+    assert wn.dtype == np.float32 and np.array_equal(wn, wavenumbers(n).astype(np.float32))
+    assert np.array_equal(wn.view(np.uint32), wo.wn_f32(n).view(np.uint32))
+    assert np.array_equal(pkg.dealiasMaskTable(n).astype(bool), dealias_mask(n))
+
+
+# ---------------------------------------------------------------- FFT at every size
+@pytest.mark.parametrize("n", SIZES)
+def test_fft2_matches_numpy(pkg, n):
+    rng = np.random.default_rng(n)
+    a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.setBuffer("packB", a)
+        s.fft.forward(None, "packB")
+        fwd = s.getBuffer("packB")
+        ref = np.fft.fft2(a.astype(np.complex128))
+        assert rel_l2(fwd, ref) <= 2e-7 * np.log2(n) + 5e-7
+        s.fft.inverse(None, "packB")
+        back = s.getBuffer("packB")
+        assert rel_l2(back, a) <= 2e-7 * np.log2(n) + 5e-7
+    finally:
+        s.destroy()
+
+
+def test_fft_unregistered_buffer_throws(pkg):
+    s = pkg.Solver.create(n=64, dyeScale=1)
+    try:
+        with pytest.raises(pkg.S2DError) as ei:
+            s.fft.forward(None, "state0")
+        assert ei.value.status == -6                                   # fft.js:84
+    finally:
+        s.destroy()
+
+
+# ---------------------------------------------------------------- fused step vs FP64 oracle
+CASES = [
+    # n, beta, mu, nu_h, p, dt, amplitude
+    (64, 5.0, 0.01, 1e-12, 4, 0.01, 2.0),
+    (128, 12.0, 0.0, 0.0, 4, 2e-3, 6.0),
+    (256, 0.0, 0.0, 1e-3, 1, 2e-3, 1.0),
+    (512, 10.0, 5e-3, 1e-20, 4, 1e-3, 8.0),
+    (1024, 0.0, 1e-2, 1e-16, 4, 1e-3, 8.0),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"n{c[0]}" for c in CASES])
+def test_fused_step_vs_oracle(pkg, case):
+    n, beta, mu, nu_h, p, dt, amp = case
+    ref = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
+    ref.set_vorticity(random_field(n, k0=n / 8, seed=n, amplitude=amp))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(beta=beta, drag=mu, viscosity=rate_for(nu_h, n, p), hyperP=p))
+        load_state(s, w_in)
+        set_fixed_dt(s, dt)
+        s.setSplats([])
+        s.encodeStep()
+        ref.step(dt=dt)
+        err1 = rel_l2(current_state(s), ref.w)
+        assert err1 <= 1e-5, f"one step rel L2 {err1:.3e}"
+        for _ in range(4):
+            s.encodeStep()
+            ref.step(dt=dt)
+        err5 = rel_l2(current_state(s), ref.w)
+        assert err5 <= 3e-5, f"five steps rel L2 {err5:.3e}"
+    finally:
+        s.destroy()
+
+
+def test_graph_replay_is_bitwise_identical(pkg):
+    n = 256
+    w = random_field(n, k0=20, seed=3, amplitude=4.0)
+    outs = []
+    for graph in (False, True):
+        s = pkg.Solver.create(n=n, dyeScale=1)
+        try:
+            s.configure(config(viscosity=1.0, hyperP=4, forceAmp=0.1, forceK=30.0, forceWidth=2.0,
+                               cfl=0.5, dtMax=2e-3))
+            s.reset({"field": w, "dyePattern": "bands"})
+            s.step(7, dye=True, reduce=True, graph=graph)
+            outs.append((current_state(s), s.currentDye, s.getBuffer("dt")))
+        finally:
+            s.destroy()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
+
+
+# ---------------------------------------------------------------- Taylor-Green invariants
+@pytest.mark.parametrize("n", [64, 256, 512])
+def test_taylor_green_jacobian_vanishes(pkg, n):
+    xs = np.arange(n) * 2 * np.pi / n
+    gx, gy = np.meshgrid(xs, xs, indexing="xy")
+    field = 6.0 * np.cos(2 * gx) * np.cos(2 * gy)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=0.0, hyperP=1))
+        s.seedPhysical(field)
+        w = current_state(s)
+        s.setBuffer("force", np.zeros((n, n), np.complex64))
+        s.velocityPack(0)
+        s.fft.inverse(None, "packA")
+        s.fft.inverse(None, "packB")
+        s.nlPack()
+        s.fft.forward(None, "physZ")
+        s.assemble()
+        nl = np.max(np.abs(s.getBuffer("rhs"))) / np.max(np.abs(w))
+        assert nl <= 2e-6, f"Jacobian/|w| = {nl:.3e}"                       # FP32 round-off
+    finally:
+        s.destroy()
+
+
+@pytest.mark.parametrize("n", [64, 512])
+def test_taylor_green_decay_rate(pkg, n):
+    nu, dt, steps = 1e-3, 2e-3, 500
+    xs = np.arange(n) * 2 * np.pi / n
+    gx, gy = np.meshgrid(xs, xs, indexing="xy")
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=rate_for(nu, n, 1), hyperP=1))
+        s.seedPhysical(6.0 * np.cos(2 * gx) * np.cos(2 * gy))
+        w0 = current_state(s)[2, 2]
+        set_fixed_dt(s, dt)
+        for _ in range(steps):
+            s.encodeStep()
+        w1 = current_state(s)[2, 2]
+        nu_h = s.paramsF[2]
+        expected = np.exp(-float(nu_h) * 8.0 * dt * steps)
+        assert abs(abs(w1 / w0) / expected - 1) <= 1e-5
+    finally:
+        s.destroy()
+
+
+def test_inviscid_invariants(pkg):
+    n, dt = 128, 2e-3
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(beta=12.0, viscosity=0.0, hyperP=4))
+        s.seedPhysical(random_field(n, k0=10, seed=2))
+        s.encodeDiagnostics(); s.copyDiagnostics()
+        d0 = s.readDiagnostics()
+        set_fixed_dt(s, dt)
+        for _ in range(200):
+            s.encodeStep()
+        s.encodeDiagnostics(); s.copyDiagnostics()
+        d1 = s.readDiagnostics()
+        assert abs(d1["energy"] / d0["energy"] - 1) <= 2e-5
+        assert abs(d1["enstrophy"] / d0["enstrophy"] - 1) <= 2e-5
+    finally:
+        s.destroy()
+
+
+# ---------------------------------------------------------------- forcing
+def test_stochastic_forcing_matches_restatement(pkg):
+    n, dt = 128, 1e-3
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        for k in range(3):
+            s.configure(config(forceAmp=0.1, forceK=20.0, forceWidth=2.0))
+            set_fixed_dt(s, dt)
+            s.setBuffer("physZ", np.zeros((n, n), np.complex64))
+            s.setBuffer("force", np.zeros((n, n), np.complex64))
+            s.assemble()
+            want = wo.stochastic_forcing(n, 0.1, 20.0, 2.0, step_index=s.stepIndex, dt=dt)
+            got = s.getBuffer("rhs")
+            assert np.count_nonzero(want) > 0
+            assert np.array_equal(got != 0, want != 0)
+            assert rel_linf(got, want) <= 2e-6
+            s.encodeStep()                      # advances stepIndex, latched at the next configure
+    finally:
+        s.destroy()
+
+
+def test_stochastic_forcing_in_fused_step(pkg):
+    n, dt = 128, 1e-3
+    w = random_field(n, k0=12, seed=9, amplitude=3.0)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=1.0, hyperP=4, forceAmp=0.1, forceK=24.0, forceWidth=2.0))
+        s.seedPhysical(w)
+        w_in = current_state(s)
+        set_fixed_dt(s, dt)
+        forcing = wo.stochastic_forcing(n, 0.1, 24.0, 2.0, step_index=0, dt=dt).astype(np.complex128)
+        ref = SpectralOracle(n=n, nu_h=float(s.paramsF[2]), hyper_p=4)
+        ref.w = w_in.astype(np.complex128)
+        ref.step(dt=dt, forcing=forcing)
+        s.encodeStep()
+        assert rel_l2(current_state(s), ref.w) <= 1e-5
+    finally:
+        s.destroy()
+
+
+def _splat(x, y, dx, dy, color=(1.0, 0.5, 0.25), radius=0.05, amp=400.0, dye=0.8):
+    return {"x": x, "y": y, "dx": dx, "dy": dy, "color": color, "radius": radius, "amp": amp, "dyeAmp": dye}
+
+
+def _splat_np(sp):
+    r = np.zeros(1, wo.SPLAT_DTYPE)[0]
+    r["x"], r["y"], r["dx"], r["dy"] = sp["x"], sp["y"], sp["dx"], sp["dy"]
+    r["r"], r["g"], r["b"] = sp["color"]
+    r["radius"], r["amp"], r["dye_amp"] = sp["radius"], sp["amp"], sp["dyeAmp"]
+    return r
+
+
+def test_pointer_force_spectrum(pkg):
+    n = 128
+    splats = [_splat(0.3, 0.6, 0.01, -0.02), _splat(0.95, 0.02, -0.015, 0.01, radius=0.08)]
+    splats += [_splat(0.1 * i, 0.5, 0.01, 0.01) for i in range(1, 9)]     # 10 given, 8 used
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=0.0))
+        s.seedPhysical(np.zeros((n, n)))
+        set_fixed_dt(s, 1e-3)
+        s.setSplats(splats)
+        s.encodeStep()
+        got = s.getBuffer("force")
+        want = np.fft.fft2(wo.pointer_force(n, [_splat_np(p) for p in splats[:8]]).astype(np.float64))
+        assert rel_l2(got, want) <= 1e-5
+        # with a zero initial state, one step equals the oracle step driven by that forcing
+        ref = SpectralOracle(n=n)
+        ref.step(dt=1e-3, forcing=want * dealias_mask(n))
+        assert rel_l2(current_state(s), ref.w) <= 1e-5
+    finally:
+        s.destroy()
+
+
+# ---------------------------------------------------------------- CFL reduction
+def test_prime_cfl_dt(pkg):
+    n = 256
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(cfl=0.5, dtMin=1e-5, dtMax=0.02))
+        s.seedPhysical(random_field(n, k0=20, seed=4, amplitude=8.0))
+        w = current_state(s)
+        s.encodePrime()
+        dt, speed = s.getBuffer("dt")[:2]
+        ref = SpectralOracle(n=n, cfl=0.5, dt_max=0.02)
+        ref.w = w.astype(np.complex128)
+        u, v = ref.velocity()
+        want_speed = np.max(np.abs(u) + np.abs(v))
+        assert abs(speed / want_speed - 1) <= 2e-6
+        want_dt, _ = wo.cfl_dt(u.astype(np.float32), v.astype(np.float32), n, 0.5, 1e-5, 0.02)
+        assert abs(dt / want_dt - 1) <= 2e-6
+        vel = s.getBuffer("vel")
+        assert rel_l2(vel.real + 0j, u) <= 1e-6 and rel_l2(vel.imag + 0j, v) <= 1e-6
+    finally:
+        s.destroy()
+
+
+def test_adaptive_step_loop_reduces_each_substep(pkg):
+    n = 128
+    s = pkg.Solver.create(n=n, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMin=1e-5, dtMax=0.02))
+        s.reset({"k0": 14, "amplitude": 6, "seed": 1})
+        s.step(3, dye=True, reduce=True)
+        vel = s.getBuffer("vel")
+        want, _ = wo.cfl_dt(vel.real.astype(np.float32), vel.imag.astype(np.float32), n, 0.5, 1e-5, 0.02)
+        assert abs(s.getBuffer("dt")[0] / want - 1) <= 1e-6
+        assert s.stepIndex == 3 and s.dyeParity == 1 and s.primed
+    finally:
+        s.destroy()
+
+
+# ---------------------------------------------------------------- seeding
+@pytest.mark.parametrize("n", [64, 256])
+def test_fill_spectrum_seed(pkg, n):
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.seed(k0=14, amplitude=6, seed=1)
+        got = s.getBuffer("state0")
+        want = wo.fill_spectrum(n, 14, 6.0, 1)
+        assert rel_linf(got, want) <= 1e-6
+        assert np.array_equal(got != 0, want != 0)
+        assert np.all(s.getBuffer("state1") == 0) and s.phase == 0
+    finally:
+        s.destroy()
+
+
+def test_seed_physical_matches_set_vorticity(pkg):
+    n = 128
+    f = random_field(n, k0=10, seed=5, amplitude=3.0).astype(np.float32)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.seedPhysical(f)
+        ref = SpectralOracle(n=n)
+        ref.set_vorticity(f.astype(np.float64))
+        assert rel_l2(s.getBuffer("state0"), ref.w) <= 1e-6
+    finally:
+        s.destroy()
+
+
+def test_seed_band_statistics(pkg):
+    n = 256
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.seedBand(6.0, 10.0, rms=1.0, seed=0)
+        w = s.getBuffer("state0").astype(np.complex128)
+        k = wavenumbers(n)
+        kr = np.sqrt(k[None, :] ** 2 + k[:, None] ** 2)
+        assert np.all(w[(kr < 6) | (kr > 10)] == 0)
+        assert abs(np.sqrt(np.sum(np.abs(w) ** 2)) / (n * n) - 1.0) < 1e-5
+        part = (-np.arange(n)) % n
+        assert np.max(np.abs(w - np.conj(w[np.ix_(part, part)]))) == 0
+        phys = np.fft.ifft2(w)
+        assert abs(np.std(phys.real) - 1.0) < 1e-5
+    finally:
+        s.destroy()
