@@ -77,43 +77,50 @@ __device__ __forceinline__ float2 stochastic_term(const DevParams& P, int n, int
   return make_float2(amp * c, sgn * amp * s);
 }
 
-// Integrating factor over half a step: E(dt/2) = exp(L dt/2),
-// L = -mu - nu_h k2^p + i beta kx/k2 (solver.wgsl:97-101, spectral2d.py:26)
-struct HalfFactor {
-  float mag;   // exp(Re L * dt/2)
-  float2 rot;  // exp(i Im L * dt/2)
-};
-__device__ __forceinline__ HalfFactor half_factor(const DevParams& P, float kx, float k2, float dt) {
-  HalfFactor h;
+// Integrating factor over half a step, carried as E(dt/2) - 1 so that factors
+// close to one keep their full relative precision: E = exp(L dt/2) with
+// L = -mu - nu_h k2^p + i beta kx/k2 (solver.wgsl:97-101, spectral2d.py:26).
+// exp(x) for |x| ~ 1e-5 rounded to FP32 keeps only ~3 digits of 1 - E, which
+// biases the damping by ~1e-5 per hundred steps; expm1 and the half-angle form
+// cos(t) - 1 = -2 sin^2(t/2) avoid the cancellation.
+__device__ __forceinline__ float2 half_factor_m1(const DevParams& P, float kx, float k2, float dt) {
   const float re = -P.mu - P.nu_h * powi(k2, P.hyper_p);
-  h.mag = expf(re * (0.5f * dt));
-  if (P.beta != 0.f) {
-    const float im = P.beta * kx / k2;
-    float s, c;
-    sincosf(im * (0.5f * dt), &s, &c);
-    h.rot = make_float2(c, s);
-  } else {
-    h.rot = make_float2(1.f, 0.f);
-  }
-  return h;
+  const float d = expm1f(re * (0.5f * dt));
+  if (P.beta == 0.f) return make_float2(d, 0.f);
+  const float th = P.beta * kx / k2 * (0.5f * dt);
+  float sh, ch;
+  sincosf(0.5f * th, &sh, &ch);
+  const float g = -2.f * sh * sh;         // cos(th) - 1
+  const float sn = 2.f * sh * ch;         // sin(th)
+  return make_float2(d + g + d * g, (1.f + d) * sn);
 }
 
-// wout = cA E(a dt) w0 + cB E(b dt) (wcur + dt rhs) for stage s, using
-// E(dt) = E(dt/2)^2 and E(-dt/2) = 1/E(dt/2) (one exp and one sincos per cell).
+// (1 + e) * w without forming 1 + e; a zero w stays zero even when e overflows
+// (the reference's E * 0 with E = inf gives NaN at modes outside the band).
+__device__ __forceinline__ float2 apply_m1(float2 e, float2 w) {
+  if (w.x == 0.f && w.y == 0.f) return w;
+  const float2 ew = cmul(e, w);
+  return make_float2(w.x + ew.x, w.y + ew.y);
+}
+
+// wout = cA E(a dt) w0 + cB E(b dt) (wcur + dt rhs) for stage s, from e = E(dt/2) - 1:
+// E(dt) - 1 = e (2 + e), E(-dt/2) - 1 = -e / (1 + e)  (one expm1 and one sincos per cell).
 template <int S>
-__device__ __forceinline__ float2 rk_update(const HalfFactor& h, float2 w0, float2 wcur, float2 rhs, float dt) {
+__device__ __forceinline__ float2 rk_update(float2 e, float2 w0, float2 wcur, float2 rhs, float dt) {
   const float2 adv = make_float2(wcur.x + dt * rhs.x, wcur.y + dt * rhs.y);
-  const float2 e_half = cscale(h.rot, h.mag);
   if constexpr (S == 0) {
-    const float2 e_full = cscale(cmul(h.rot, h.rot), h.mag * h.mag);
-    return cmul(e_full, adv);
+    const float2 full = cmul(e, make_float2(2.f + e.x, e.y));
+    return apply_m1(full, adv);
   } else if constexpr (S == 1) {
-    const float2 e_mhalf = cscale(cconj(h.rot), 1.f / h.mag);
-    const float2 a = cmul(e_half, w0), b = cmul(e_mhalf, adv);
+    const float2 one_e = make_float2(1.f + e.x, e.y);
+    const float den = one_e.x * one_e.x + one_e.y * one_e.y;
+    const float2 q = cmul(e, cconj(one_e));
+    const float2 mhalf = make_float2(-q.x / den, -q.y / den);
+    const float2 a = apply_m1(e, w0), b = apply_m1(mhalf, adv);
     return make_float2(0.75f * a.x + 0.25f * b.x, 0.75f * a.y + 0.25f * b.y);
   } else {
-    const float2 e_full = cscale(cmul(h.rot, h.rot), h.mag * h.mag);
-    const float2 a = cmul(e_full, w0), b = cmul(e_half, adv);
+    const float2 full = cmul(e, make_float2(2.f + e.x, e.y));
+    const float2 a = apply_m1(full, w0), b = apply_m1(e, adv);
     return make_float2((1.f / 3.f) * a.x + (2.f / 3.f) * b.x, (1.f / 3.f) * a.y + (2.f / 3.f) * b.y);
   }
 }

@@ -256,8 +256,7 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
         if (k2 == 0.f) {
           w = make_float2(0.f, 0.f);
         } else {
-          const HalfFactor hf = half_factor(P, kx, k2, dt);
-          w = rk_update<MODE>(hf, w0, wc, rhs, dt);
+          w = rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
         }
         a.wout[o] = w;
       }
@@ -383,8 +382,7 @@ __global__ void k_rk3(const float2* __restrict__ w0, const float2* __restrict__ 
     return;
   }
   const float dt = dtbuf[0];
-  const HalfFactor hf = half_factor(*params, kx, k2, dt);
-  wout[idx] = rk_update<S>(hf, w0[idx], wcur[idx], rhs[idx], dt);
+  wout[idx] = rk_update<S>(half_factor_m1(*params, kx, k2, dt), w0[idx], wcur[idx], rhs[idx], dt);
 }
 
 }  // namespace s2d

@@ -64,7 +64,7 @@ CASES = [
     (128, 12.0, 0.0, 0.0, 4, 2e-3, 6.0),
     (256, 0.0, 0.0, 1e-3, 1, 2e-3, 1.0),
     (512, 10.0, 5e-3, 1e-20, 4, 1e-3, 8.0),
-    (1024, 0.0, 1e-2, 1e-16, 4, 1e-3, 8.0),
+    (1024, 0.0, 1e-2, 1.0 / (1024 / 3.0) ** 8, 4, 1e-3, 8.0),
 ]
 
 
@@ -90,6 +90,30 @@ def test_fused_step_vs_oracle(pkg, case):
             ref.step(dt=dt)
         err5 = rel_l2(current_state(s), ref.w)
         assert err5 <= 3e-5, f"five steps rel L2 {err5:.3e}"
+    finally:
+        s.destroy()
+
+
+def test_out_of_band_overflow_is_contained(pkg):
+    """E(-dt/2) = exp(+205) beyond the dealias band overflows in FP32; the reference
+    shader forms inf * 0 = NaN there (solver.wgsl:121).  Zero modes must stay zero and
+    the step must match the FP64 oracle, whose factor does not overflow."""
+    n, dt, rate = 256, 1e-3, 1000.0
+    ref = SpectralOracle(n=n, nu_h=rate / (n / 3.0) ** 8, hyper_p=4)
+    ref.set_vorticity(random_field(n, k0=20, seed=6, amplitude=4.0))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=rate, hyperP=4))
+        load_state(s, w_in)
+        set_fixed_dt(s, dt)
+        s.encodeStep()
+        ref.step(dt=dt)
+        got = current_state(s)
+        assert np.all(np.isfinite(got))
+        assert np.all(got[~dealias_mask(n)] == 0)
+        assert rel_l2(got, ref.w) <= 1e-5
     finally:
         s.destroy()
 
@@ -132,7 +156,9 @@ def test_taylor_green_jacobian_vanishes(pkg, n):
         s.fft.forward(None, "physZ")
         s.assemble()
         nl = np.max(np.abs(s.getBuffer("rhs"))) / np.max(np.abs(w))
-        assert nl <= 2e-6, f"Jacobian/|w| = {nl:.3e}"                       # FP32 round-off
+        # FP32 round-off of the u*omega transforms (O(|omega| |u|) products, ~1e-7 per
+        # pass, growing with log N) relative to the spectral amplitude of omega
+        assert nl <= 1e-5, f"Jacobian/|w| = {nl:.3e}"
     finally:
         s.destroy()
 
@@ -269,7 +295,9 @@ def test_prime_cfl_dt(pkg):
         want_dt, _ = wo.cfl_dt(u.astype(np.float32), v.astype(np.float32), n, 0.5, 1e-5, 0.02)
         assert abs(dt / want_dt - 1) <= 2e-6
         vel = s.getBuffer("vel")
-        assert rel_l2(vel.real + 0j, u) <= 1e-6 and rel_l2(vel.imag + 0j, v) <= 1e-6
+        # u shares one complex transform with omega (two-for-one packing, solver.wgsl:38),
+        # so its error is the transform's round-off scaled by |omega| / |u| (~16 here)
+        assert rel_l2(vel.real + 0j, u) <= 5e-6 and rel_l2(vel.imag + 0j, v) <= 1e-6
     finally:
         s.destroy()
 
