@@ -157,6 +157,9 @@ int s2d_seed_band(s2d_solver* s, float kmin, float kmax, float rms, uint32_t see
 int s2d_encode_prime(s2d_solver* s);                                     /* solver.js:475-486 */
 int s2d_encode_step(s2d_solver* s);                                      /* solver.js:488-521 */
 int s2d_encode_dye(s2d_solver* s);                                       /* solver.js:523-536 */
+/* encodeDye as the reference's three separate dispatches (advect_fwd, advect_back,
+ * advect_corr, dye.wgsl:58-113); same result bits as s2d_encode_dye. */
+int s2d_encode_dye_passes(s2d_solver* s);
 int s2d_encode_reduce(s2d_solver* s);                                    /* solver.js:538-545 */
 /* `substeps` repetitions of encodeStep (+ encodeDye, + encodeReduce per flags),
  * priming first when needed: the body of main.js:409-419. */
@@ -207,8 +210,10 @@ int s2d_set_dye(s2d_solver* s, const uint16_t* in);
 #define S2D_PROF_FORCE 3
 #define S2D_PROF_OTHER 4
 #define S2D_PROF_CLASSES 5
-/* enable != 0 starts recording a CUDA event pair around every kernel the
- * non-graph entry points launch (no reference counterpart); 0 stops. */
+/* enable != 0 starts recording a CUDA event pair around every kernel class the
+ * step entry points launch (no reference counterpart); 0 stops.  With
+ * s2d_step_graph the events are nodes of the captured graph and each replay is
+ * synchronized and read, so the times are device times without host gaps. */
 int s2d_profile(s2d_solver* s, int enable);
 /* Synchronizes, then returns the summed device time (ms) and launch count per
  * class since the last read, and clears them. */

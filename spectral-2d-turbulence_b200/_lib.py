@@ -96,6 +96,7 @@ PROTOTYPES = {
     "s2d_encode_prime": (_i, [_vp]),
     "s2d_encode_step": (_i, [_vp]),
     "s2d_encode_dye": (_i, [_vp]),
+    "s2d_encode_dye_passes": (_i, [_vp]),
     "s2d_encode_reduce": (_i, [_vp]),
     "s2d_step": (_i, [_vp, _i, C.c_uint]),
     "s2d_step_graph": (_i, [_vp, _i, C.c_uint]),

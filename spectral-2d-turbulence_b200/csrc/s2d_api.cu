@@ -111,10 +111,18 @@ static int check_device(int dev) {
 struct GraphKey {
   int phase, slot, parity;
   unsigned flags;
-  int ptr;
+  int ptr, prof;
   bool operator<(const GraphKey& o) const {
-    return std::tie(phase, slot, parity, flags, ptr) < std::tie(o.phase, o.slot, o.parity, o.flags, o.ptr);
+    return std::tie(phase, slot, parity, flags, ptr, prof) <
+           std::tie(o.phase, o.slot, o.parity, o.flags, o.ptr, o.prof);
   }
+};
+
+// a captured substep; when profiling, it carries event-record nodes around its kernels
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> events;
 };
 
 struct s2d_solver {
@@ -150,10 +158,12 @@ struct s2d_solver {
   double sim_time = 0.0;
   bool primed = false, packs_valid = false, reduced_valid = false, disposed = false;
   int read_state = 0;  // 0 idle, 1 copied
-  std::map<GraphKey, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+  std::map<GraphKey, GraphEntry> graphs;
   // instrumentation: event pairs around launches, by kernel class
   bool profiling = false;
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> prof_events;
+  double prof_ms[S2D_PROF_CLASSES] = {0};
+  int prof_cnt[S2D_PROF_CLASSES] = {0};
 };
 
 // RAII event pair around the launches of one kernel class (when profiling)
@@ -177,8 +187,12 @@ static int seed_parts_count(int n) { return (n * n + 255) / 256; }
 
 static void free_solver(s2d_solver* s) {
   for (auto& kv : s->graphs) {
-    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
-    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    for (auto& ev : kv.second.events) {
+      cudaEventDestroy(std::get<1>(ev));
+      cudaEventDestroy(std::get<2>(ev));
+    }
   }
   s->graphs.clear();
   for (auto& ev : s->prof_events) {
@@ -357,6 +371,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMallocHost(&s->h_zonal, sizeof(float) * n), "pinned zonal");
   TRY(cudaMallocHost(&s->h_dt, sizeof(float) * 4), "pinned dt");
   TRY(ops->set_attrs(), "kernel attributes");
+  TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
   // zero everything the reference's fresh buffers hold as zero
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
   TRY(cudaMemsetAsync(s->packA, 0, cbytes, s->stream), "memset");
@@ -589,18 +605,36 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
   return S2D_OK;
 }
 
+static uint2* tex(s2d_solver* s, int i) { return reinterpret_cast<uint2*>(s->dye[i]); }
+
+// encodeDye (solver.js:523-536) as one fused launch: forward, backward and
+// corrected passes of a tile computed from on-chip halos (s2d_dye.cuh)
 extern "C" int s2d_encode_dye(s2d_solver* s) {
+  S2D_USE(s);
+  DeviceGuard guard(s->dev);
+  const int p = s->dye_parity, m = s->m;
+  const dim3 grd((m + kDyeTile - 1) / kDyeTile, (m + kDyeTile - 1) / kDyeTile);
+  ProfScope ps(s, S2D_PROF_DYE);
+  k_dye_fused<<<grd, kDyeThreads, dye_fused_smem(s->n, m), s->stream>>>(
+      s->vel, tex(s, p), tex(s, 1 - p), dt_slot(s, s->slot), s->dparams, s->dsplats, s->n, m);
+  S2D_LAUNCHED();
+  s->dye_parity = 1 - p;
+  return S2D_OK;
+}
+
+// the reference's three dispatches advect_fwd, advect_back, advect_corr (solver.js:523-536)
+extern "C" int s2d_encode_dye_passes(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
   const int p = s->dye_parity, m = s->m;
   const dim3 blk(16, 16), grd((m + 15) / 16, (m + 15) / 16);
   const float* dt = dt_slot(s, s->slot);
   ProfScope ps(s, S2D_PROF_DYE);
-  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[p], s->dye[1 - p], dt, 1.f, s->n, m);
+  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, tex(s, p), tex(s, 1 - p), dt, 1.f, s->n, m);
   S2D_LAUNCHED();
-  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[1 - p], s->dye[2], dt, -1.f, s->n, m);
+  k_dye_advect<<<grd, blk, 0, s->stream>>>(s->vel, tex(s, 1 - p), tex(s, 2), dt, -1.f, s->n, m);
   S2D_LAUNCHED();
-  k_dye_correct<<<grd, blk, 0, s->stream>>>(s->vel, s->dye[p], s->dye[2], s->dye[1 - p], dt, s->dparams,
+  k_dye_correct<<<grd, blk, 0, s->stream>>>(s->vel, tex(s, p), tex(s, 2), tex(s, 1 - p), dt, s->dparams,
                                             s->dsplats, s->n, m);
   S2D_LAUNCHED();
   s->dye_parity = 1 - p;
@@ -666,7 +700,7 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
   if (flags & S2D_STEP_RELATCH)
     if (int rc = sync_step_counter(s)) return rc;
   for (int i = 0; i < substeps; ++i) {
-    const GraphKey key{s->phase, s->slot, s->dye_parity, flags, s->hs.count > 0 ? 1 : 0};
+    const GraphKey key{s->phase, s->slot, s->dye_parity, flags, s->hs.count > 0 ? 1 : 0, s->profiling ? 1 : 0};
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       // capture one substep from the current host state, then restore it
@@ -675,6 +709,7 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
       const bool rv = s->reduced_valid;
       cudaGraph_t g = nullptr;
       cudaGraphExec_t ge = nullptr;
+      const size_t ev_before = s->prof_events.size();
       S2D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
       int rc = (flags & S2D_STEP_RELATCH) ? enqueue_relatch(s) : S2D_OK;
       if (!rc) rc = s2d_encode_step(s);
@@ -696,9 +731,26 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
       s->dye_parity = parity;
       s->step_index = si;
       s->reduced_valid = rv;
-      it = s->graphs.emplace(key, std::make_pair(g, ge)).first;
+      GraphEntry entry;
+      entry.graph = g;
+      entry.exec = ge;
+      // event pairs recorded during capture belong to the graph's event nodes
+      entry.events.assign(s->prof_events.begin() + ev_before, s->prof_events.end());
+      s->prof_events.resize(ev_before);
+      it = s->graphs.emplace(key, std::move(entry)).first;
     }
-    S2D_CUDA(cudaGraphLaunch(it->second.second, s->stream));
+    S2D_CUDA(cudaGraphLaunch(it->second.exec, s->stream));
+    if (!it->second.events.empty()) {
+      // device times of this replay's kernels (the next replay re-records the events)
+      S2D_CUDA(cudaStreamSynchronize(s->stream));
+      for (auto& ev : it->second.events) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, std::get<1>(ev), std::get<2>(ev)) == cudaSuccess) {
+          s->prof_ms[std::get<0>(ev)] += t;
+          s->prof_cnt[std::get<0>(ev)] += 1;
+        }
+      }
+    }
     // advance the host mirror exactly as the captured substep did
     s->phase = (s->phase + 1) % 3;
     s->step_index += 1;
@@ -1032,6 +1084,12 @@ extern "C" int s2d_profile_read(s2d_solver* s, double* ms, int* launches) {
   S2D_CUDA(cudaStreamSynchronize(s->stream));
   double acc[S2D_PROF_CLASSES] = {0};
   int cnt[S2D_PROF_CLASSES] = {0};
+  for (int i = 0; i < S2D_PROF_CLASSES; ++i) {
+    acc[i] = s->prof_ms[i];
+    cnt[i] = s->prof_cnt[i];
+    s->prof_ms[i] = 0.0;
+    s->prof_cnt[i] = 0;
+  }
   for (auto& ev : s->prof_events) {
     float t = 0.f;
     if (cudaEventElapsedTime(&t, std::get<1>(ev), std::get<2>(ev)) == cudaSuccess) {

@@ -3,6 +3,7 @@
 #include <cuda_fp16.h>
 #include "s2d_band.cuh"
 #include "s2d_device.cuh"
+#include "s2d_dye.cuh"
 
 namespace s2d {
 
@@ -46,8 +47,6 @@ __global__ void k_mask_table(uint8_t* out, int n) {
 }
 
 // ------------------------------------------------------------------ pointer forcing (force.wgsl:5-27)
-__device__ __forceinline__ float wrap01(float x) { return x - floorf(x); }
-__device__ __forceinline__ float sepf(float a, float b) { return wrap01(a - b + 0.5f) - 0.5f; }
 
 __global__ void k_pointer_force(float2* force, const DevSplats* __restrict__ S, int n) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -314,121 +313,6 @@ __global__ void k_paint_bands(ushort4* dye, int m) {
   uint16_t c[3];
   for (int k = 0; k < 3; ++k) c[k] = to_half_trunc((float)(band * (warm[k] * mix + cool[k] * (1.0 - mix)) * 0.9));
   dye[idx] = make_ushort4(c[0], c[1], c[2], to_half_trunc(1.0f));
-}
-
-struct Rgba {
-  float r, g, b, a;
-};
-__device__ __forceinline__ Rgba load_texel(const ushort4* __restrict__ t, int x, int y, int m) {
-  const ushort4 u = __ldg(t + (size_t)y * m + x);
-  return {__half2float(__ushort_as_half(u.x)), __half2float(__ushort_as_half(u.y)),
-          __half2float(__ushort_as_half(u.z)), __half2float(__ushort_as_half(u.w))};
-}
-__device__ __forceinline__ int wrapi(int i, int m) { return ((i % m) + m) % m; }
-
-// bilinear velocity at normalised p (dye.wgsl:20-38)
-__device__ __forceinline__ float2 sample_vel(const float2* __restrict__ vel, float px, float py, int n) {
-  const float nf = (float)n;
-  const float gx = px * nf - 0.5f, gy = py * nf - 0.5f;
-  const float bx = floorf(gx), by = floorf(gy);
-  const float fx = gx - bx, fy = gy - by;
-  const int ix = (int)bx, iy = (int)by;
-  const int x0 = wrapi(ix, n), x1 = wrapi(ix + 1, n), y0 = wrapi(iy, n), y1 = wrapi(iy + 1, n);
-  const float2 v00 = __ldg(vel + (size_t)y0 * n + x0), v10 = __ldg(vel + (size_t)y0 * n + x1);
-  const float2 v01 = __ldg(vel + (size_t)y1 * n + x0), v11 = __ldg(vel + (size_t)y1 * n + x1);
-  const float ax = v00.x * (1.f - fx) + v10.x * fx, ay = v00.y * (1.f - fx) + v10.y * fx;
-  const float bx2 = v01.x * (1.f - fx) + v11.x * fx, by2 = v01.y * (1.f - fx) + v11.y * fx;
-  return make_float2(ax * (1.f - fy) + bx2 * fy, ay * (1.f - fy) + by2 * fy);
-}
-
-// midpoint back-trace (dye.wgsl:40-45)
-__device__ __forceinline__ float2 trace_pos(const float2* __restrict__ vel, float px, float py, float h, int n) {
-  const float2 v1 = sample_vel(vel, px, py, n);
-  float mx = px - 0.5f * (v1.x * h) + 1.f, my = py - 0.5f * (v1.y * h) + 1.f;
-  mx -= floorf(mx);
-  my -= floorf(my);
-  const float2 v2 = sample_vel(vel, mx, my, n);
-  float sx = px - v2.x * h + 1.f, sy = py - v2.y * h + 1.f;
-  return make_float2(sx - floorf(sx), sy - floorf(sy));
-}
-
-// software form of a linear-filtered, repeat-addressed texture sample
-__device__ __forceinline__ Rgba sample_dye(const ushort4* __restrict__ tex, float sx, float sy, int m,
-                                           Rgba* lo = nullptr, Rgba* hi = nullptr) {
-  const float mf = (float)m;
-  const float gx = sx * mf - 0.5f, gy = sy * mf - 0.5f;
-  const float bx = floorf(gx), by = floorf(gy);
-  const float fx = gx - bx, fy = gy - by;
-  const int x0 = wrapi((int)bx, m), x1 = wrapi((int)bx + 1, m);
-  const int y0 = wrapi((int)by, m), y1 = wrapi((int)by + 1, m);
-  const Rgba c00 = load_texel(tex, x0, y0, m), c10 = load_texel(tex, x1, y0, m);
-  const Rgba c01 = load_texel(tex, x0, y1, m), c11 = load_texel(tex, x1, y1, m);
-  auto lerp2 = [&](float a00, float a10, float a01, float a11) {
-    const float a = a00 * (1.f - fx) + a10 * fx, b = a01 * (1.f - fx) + a11 * fx;
-    return a * (1.f - fy) + b * fy;
-  };
-  if (lo) {
-    lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
-    lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
-    lo->b = fminf(fminf(c00.b, c10.b), fminf(c01.b, c11.b));
-    hi->r = fmaxf(fmaxf(c00.r, c10.r), fmaxf(c01.r, c11.r));
-    hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
-    hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
-  }
-  return {lerp2(c00.r, c10.r, c01.r, c11.r), lerp2(c00.g, c10.g, c01.g, c11.g),
-          lerp2(c00.b, c10.b, c01.b, c11.b), lerp2(c00.a, c10.a, c01.a, c11.a)};
-}
-
-__device__ __forceinline__ ushort4 pack_rgba(float r, float g, float b, float a) {
-  return make_ushort4(__half_as_ushort(__float2half_rn(r)), __half_as_ushort(__float2half_rn(g)),
-                      __half_as_ushort(__float2half_rn(b)), __half_as_ushort(__float2half_rn(a)));
-}
-
-// advect_fwd / advect_back (dye.wgsl:58-74): dst = src sampled at trace(p, sign*dt/2pi)
-__global__ void k_dye_advect(const float2* __restrict__ vel, const ushort4* __restrict__ src, ushort4* dst,
-                             const float* __restrict__ dtbuf, float sign, int n, int m) {
-  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
-  if (gx >= m || gy >= m) return;
-  const float mf = (float)m;
-  const float px = ((float)gx + 0.5f) / mf, py = ((float)gy + 0.5f) / mf;
-  const float h = sign * dtbuf[0] / kTwoPiF;
-  const float2 s = trace_pos(vel, px, py, h, n);
-  const Rgba c = sample_dye(src, s.x, s.y, m);
-  dst[(size_t)gy * m + gx] = pack_rgba(c.r, c.g, c.b, c.a);
-}
-
-// advect_corr (dye.wgsl:76-113): BFECC correction, MacCormack clamp, fade, splat dye
-__global__ void k_dye_correct(const float2* __restrict__ vel, const ushort4* __restrict__ src,
-                              const ushort4* __restrict__ aux, ushort4* dst, const float* __restrict__ dtbuf,
-                              const DevParams* __restrict__ params, const DevSplats* __restrict__ S, int n,
-                              int m) {
-  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
-  if (gx >= m || gy >= m) return;
-  const float mf = (float)m;
-  const float px = ((float)gx + 0.5f) / mf, py = ((float)gy + 0.5f) / mf;
-  const float h = dtbuf[0] / kTwoPiF;
-  const float2 s = trace_pos(vel, px, py, h, n);
-  Rgba lo, hi;
-  const Rgba a = sample_dye(src, s.x, s.y, m, &lo, &hi);
-  const Rgba b = sample_dye(aux, s.x, s.y, m);
-  const float fade = params->dye_fade;
-  float r = fminf(fmaxf(1.5f * a.r - 0.5f * b.r, lo.r), hi.r) * fade;
-  float g = fminf(fmaxf(1.5f * a.g - 0.5f * b.g, lo.g), hi.g) * fade;
-  float bb = fminf(fmaxf(1.5f * a.b - 0.5f * b.b, lo.b), hi.b) * fade;
-  const int cnt = S->count;
-  for (int i = 0; i < cnt; ++i) {
-    const DevSplat sp = S->items[i];
-    const float rx = sepf(px, sp.x), ry = sepf(py, sp.y);
-    const float sig2 = fmaxf(sp.radius * sp.radius, 1e-8f);
-    const float r2 = rx * rx + ry * ry;
-    if (r2 < 9.f * sig2) {
-      const float wgt = sp.dye_amp * expf(-r2 / sig2);
-      r += sp.r * wgt;
-      g += sp.g * wgt;
-      bb += sp.b * wgt;
-    }
-  }
-  dst[(size_t)gy * m + gx] = pack_rgba(r, g, bb, 1.f);
 }
 
 }  // namespace s2d

@@ -119,9 +119,11 @@ __device__ __forceinline__ float2 rk_update(float2 e, float2 w0, float2 wcur, fl
     const float2 a = apply_m1(e, w0), b = apply_m1(mhalf, adv);
     return make_float2(0.75f * a.x + 0.25f * b.x, 0.75f * a.y + 0.25f * b.y);
   } else {
+    // 1/3 a + 2/3 b as b + (a - b)/3: the FP32 constants 1/3 and 2/3 both round up
+    // (their sum is 1 + 3e-8), which would bias every step; on (a - b) the bias vanishes
     const float2 full = cmul(e, make_float2(2.f + e.x, e.y));
     const float2 a = apply_m1(full, w0), b = apply_m1(e, adv);
-    return make_float2((1.f / 3.f) * a.x + (2.f / 3.f) * b.x, (1.f / 3.f) * a.y + (2.f / 3.f) * b.y);
+    return make_float2(b.x + (a.x - b.x) * (1.f / 3.f), b.y + (a.y - b.y) * (1.f / 3.f));
   }
 }
 
@@ -135,6 +137,10 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// periodic helpers of common.wgsl:42-48
+__device__ __forceinline__ float wrap01(float x) { return x - floorf(x); }
+__device__ __forceinline__ float sepf(float a, float b) { return wrap01(a - b + 0.5f) - 0.5f; }
 
 // CFL dt from the maximum of |u|+|v| (reduce.wgsl:54-62)
 __device__ __forceinline__ float cfl_dt(const DevParams& P, float speed) {

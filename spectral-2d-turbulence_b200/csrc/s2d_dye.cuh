@@ -1,0 +1,334 @@
+// s2d_dye.cuh -- BFECC + MacCormack-limited semi-Lagrangian dye advection (dye.wgsl).
+//
+// The dye is M x M rgba16float texels (ushort4 of binary16 bits) on a grid
+// refined dyeScale times over the N x N velocity grid.  Texture filtering is
+// restated in software: repeat-wrapped bilinear in FP32 (the reference samples
+// with a linear-filtered, repeat-addressed sampler).
+//
+// Two implementations share every sampling function, so they agree bit for bit:
+//   * three passes (advect_fwd, advect_back, advect_corr) exactly as the
+//     reference dispatches them, each reading and writing whole textures;
+//   * k_dye_fused: one launch per step.  A CTA owns a 32 x 32 output tile and
+//     keeps, in shared memory, the source texels of the tile plus a 3-level halo,
+//     the forward-pass texels of the tile plus 2 levels and the backward-pass
+//     texels plus 1 level; each level's halo (2 texels) covers the bilinear
+//     footprint of a back-trace of up to one texel, which the CFL limit gives at
+//     dyeScale 2.  A sample outside the on-chip region is recomputed from global
+//     memory (the forward/backward values at that texel are re-derived), so the
+//     result does not depend on the halo being large enough.  Texture traffic
+//     drops from 7 texture passes to one read and one write.
+#pragma once
+#include <cuda_fp16.h>
+#include "s2d_device.cuh"
+
+namespace s2d {
+
+struct Rgba {
+  float r, g, b, a;
+};
+
+__device__ __forceinline__ Rgba unpack_texel(uint2 u) {
+  const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  const float2 ba = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+  return {rg.x, rg.y, ba.x, ba.y};
+}
+__device__ __forceinline__ uint2 pack_texel(float r, float g, float b, float a) {
+  const __half2 rg = __floats2half2_rn(r, g), ba = __floats2half2_rn(b, a);
+  return make_uint2(*reinterpret_cast<const unsigned*>(&rg), *reinterpret_cast<const unsigned*>(&ba));
+}
+__device__ __forceinline__ Rgba round_texel(const Rgba& c) { return unpack_texel(pack_texel(c.r, c.g, c.b, c.a)); }
+
+// ---------------------------------------------------------------- fetchers
+struct GlobalTex {
+  const uint2* t;
+  int m;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const { return unpack_texel(__ldg(t + (size_t)y * m + x)); }
+};
+struct GlobalVel {
+  const float2* v;
+  int n;
+  __device__ __forceinline__ float2 operator()(int x, int y) const { return __ldg(v + (size_t)y * n + x); }
+};
+
+// Every operation below is an explicitly rounded intrinsic (no multiply-add
+// contraction), so the fused and the three-pass kernels produce the same bits.
+__device__ __forceinline__ float lerp1(float a, float b, float t) {
+  return __fadd_rn(__fmul_rn(a, __fsub_rn(1.f, t)), __fmul_rn(b, t));   // WGSL mix(a, b, t)
+}
+
+// bilinear velocity at normalised p (dye.wgsl:27-38); cell indices wrapped
+template <class VF>
+__device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, int n) {
+  const float nf = (float)n;
+  const float gx = __fsub_rn(__fmul_rn(px, nf), 0.5f), gy = __fsub_rn(__fmul_rn(py, nf), 0.5f);
+  const float bx = floorf(gx), by = floorf(gy);
+  const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
+  const int ix = (int)bx, iy = (int)by;
+  const int x0 = ix & (n - 1), x1 = (ix + 1) & (n - 1), y0 = iy & (n - 1), y1 = (iy + 1) & (n - 1);
+  const float2 v00 = vf(x0, y0), v10 = vf(x1, y0), v01 = vf(x0, y1), v11 = vf(x1, y1);
+  return make_float2(lerp1(lerp1(v00.x, v10.x, fx), lerp1(v01.x, v11.x, fx), fy),
+                     lerp1(lerp1(v00.y, v10.y, fx), lerp1(v01.y, v11.y, fx), fy));
+}
+
+__device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - d + 1)
+  const float x = __fadd_rn(__fsub_rn(p, d), 1.f);
+  return __fsub_rn(x, floorf(x));
+}
+
+// midpoint back-trace (dye.wgsl:40-45)
+template <class VF>
+__device__ __forceinline__ float2 trace_pos(const VF& vf, float px, float py, float h, int n) {
+  const float2 v1 = sample_vel(vf, px, py, n);
+  const float mx = fract_shift(px, __fmul_rn(0.5f, __fmul_rn(v1.x, h)));
+  const float my = fract_shift(py, __fmul_rn(0.5f, __fmul_rn(v1.y, h)));
+  const float2 v2 = sample_vel(vf, mx, my, n);
+  return make_float2(fract_shift(px, __fmul_rn(v2.x, h)), fract_shift(py, __fmul_rn(v2.y, h)));
+}
+
+// texel footprint of a repeat-addressed linear sample at normalised s
+struct Footprint {
+  int x0, x1, y0, y1;
+  float fx, fy;
+};
+__device__ __forceinline__ Footprint footprint(float sx, float sy, int m) {
+  const float mf = (float)m;
+  const float gx = __fsub_rn(__fmul_rn(sx, mf), 0.5f), gy = __fsub_rn(__fmul_rn(sy, mf), 0.5f);
+  const float bx = floorf(gx), by = floorf(gy);
+  Footprint f;
+  f.fx = __fsub_rn(gx, bx);
+  f.fy = __fsub_rn(gy, by);
+  f.x0 = (int)bx & (m - 1);
+  f.x1 = ((int)bx + 1) & (m - 1);
+  f.y0 = (int)by & (m - 1);
+  f.y1 = ((int)by + 1) & (m - 1);
+  return f;
+}
+
+__device__ __forceinline__ float lerp2(float a00, float a10, float a01, float a11, float fx, float fy) {
+  return lerp1(lerp1(a00, a10, fx), lerp1(a01, a11, fx), fy);
+}
+
+template <class TF>
+__device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* lo = nullptr, Rgba* hi = nullptr) {
+  const Rgba c00 = tf(f.x0, f.y0), c10 = tf(f.x1, f.y0), c01 = tf(f.x0, f.y1), c11 = tf(f.x1, f.y1);
+  if (lo) {
+    lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
+    lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
+    lo->b = fminf(fminf(c00.b, c10.b), fminf(c01.b, c11.b));
+    hi->r = fmaxf(fmaxf(c00.r, c10.r), fmaxf(c01.r, c11.r));
+    hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
+    hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
+  }
+  return {lerp2(c00.r, c10.r, c01.r, c11.r, f.fx, f.fy), lerp2(c00.g, c10.g, c01.g, c11.g, f.fx, f.fy),
+          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
+}
+
+__device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
+  const float mf = (float)m;
+  return make_float2(__fdiv_rn(__fadd_rn((float)x, 0.5f), mf), __fdiv_rn(__fadd_rn((float)y, 0.5f), mf));
+}
+
+// BFECC correction of one texel from its source and back-advected samples (dye.wgsl:81-112)
+template <class SF, class BF>
+__device__ __forceinline__ uint2 correct_texel(const SF& src, const BF& back, const Footprint& f, float px, float py,
+                                               float fade, const DevSplats* __restrict__ S) {
+  Rgba lo, hi;
+  const Rgba a = bilerp(src, f, &lo, &hi);
+  const Rgba b = bilerp(back, f);
+  auto corr = [&](float x, float y, float l, float u) {
+    return __fmul_rn(fminf(fmaxf(__fsub_rn(__fmul_rn(1.5f, x), __fmul_rn(0.5f, y)), l), u), fade);
+  };
+  float r = corr(a.r, b.r, lo.r, hi.r);
+  float g = corr(a.g, b.g, lo.g, hi.g);
+  float bb = corr(a.b, b.b, lo.b, hi.b);
+  const int cnt = S->count;
+  for (int i = 0; i < cnt; ++i) {
+    const DevSplat sp = S->items[i];
+    const float rx = sepf(px, sp.x), ry = sepf(py, sp.y);
+    const float sig2 = fmaxf(__fmul_rn(sp.radius, sp.radius), 1e-8f);
+    const float r2 = __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry));
+    if (r2 < __fmul_rn(9.f, sig2)) {
+      const float wgt = __fmul_rn(sp.dye_amp, expf(-__fdiv_rn(r2, sig2)));
+      r = __fadd_rn(r, __fmul_rn(sp.r, wgt));
+      g = __fadd_rn(g, __fmul_rn(sp.g, wgt));
+      bb = __fadd_rn(bb, __fmul_rn(sp.b, wgt));
+    }
+  }
+  return pack_texel(r, g, bb, 1.f);
+}
+
+// ---------------------------------------------------------------- three passes (reference order)
+// advect_fwd / advect_back (dye.wgsl:58-74): dst = src sampled at trace(p, sign*dt/2pi)
+__global__ void k_dye_advect(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* dst,
+                             const float* __restrict__ dtbuf, float sign, int n, int m) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= m || gy >= m) return;
+  const float2 p = texel_pos(gx, gy, m);
+  const float h = __fdiv_rn(__fmul_rn(sign, dtbuf[0]), kTwoPiF);
+  const float2 s = trace_pos(GlobalVel{vel, n}, p.x, p.y, h, n);
+  const Rgba c = bilerp(GlobalTex{src, m}, footprint(s.x, s.y, m));
+  dst[(size_t)gy * m + gx] = pack_texel(c.r, c.g, c.b, c.a);
+}
+
+// advect_corr (dye.wgsl:76-113)
+__global__ void k_dye_correct(const float2* __restrict__ vel, const uint2* __restrict__ src,
+                              const uint2* __restrict__ aux, uint2* dst, const float* __restrict__ dtbuf,
+                              const DevParams* __restrict__ params, const DevSplats* __restrict__ S, int n, int m) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= m || gy >= m) return;
+  const float2 p = texel_pos(gx, gy, m);
+  const float h = __fdiv_rn(dtbuf[0], kTwoPiF);
+  const float2 s = trace_pos(GlobalVel{vel, n}, p.x, p.y, h, n);
+  dst[(size_t)gy * m + gx] =
+      correct_texel(GlobalTex{src, m}, GlobalTex{aux, m}, footprint(s.x, s.y, m), p.x, p.y, params->dye_fade, S);
+}
+
+// ---------------------------------------------------------------- fused single pass
+constexpr int kDyeTile = 32;         // output tile edge
+constexpr int kDyeHalo = 2;          // halo per level (texels)
+constexpr int kDyeThreads = 256;
+constexpr int kDyeW1 = kDyeTile + 2 * kDyeHalo;   // backward-pass region edge
+constexpr int kDyeW2 = kDyeTile + 4 * kDyeHalo;   // forward-pass region edge
+constexpr int kDyeW3 = kDyeTile + 6 * kDyeHalo;   // source region edge
+
+// velocity cells needed by traces from the forward-pass region, for an n x n velocity grid
+// under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
+__host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
+__host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
+  return sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
+         sizeof(float2) * dye_vel_edge(n, m) * dye_vel_edge(n, m);
+}
+
+// on-chip window with an exact global fallback; coordinates are wrapped grid indices
+struct SmemTex {
+  const uint2* sm;
+  int ox, oy, w, m;
+  const uint2* g;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
+    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    return unpack_texel(__ldg(g + (size_t)y * m + x));
+  }
+};
+struct SmemVel {
+  const float2* sm;
+  int ox, oy, w, n;
+  const float2* g;
+  __device__ __forceinline__ float2 operator()(int x, int y) const {
+    const int rx = (x - ox) & (n - 1), ry = (y - oy) & (n - 1);
+    if (rx < w && ry < w) return sm[ry * w + rx];
+    return __ldg(g + (size_t)y * n + x);
+  }
+};
+
+// forward pass value at texel (x, y), as the advect_fwd texture would hold it
+struct FwdEval {
+  SmemVel vel;
+  SmemTex src;
+  float h;
+  int n, m;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+    const float2 p = texel_pos(x, y, m);
+    const float2 s = trace_pos(vel, p.x, p.y, h, n);
+    return round_texel(bilerp(src, footprint(s.x, s.y, m)));
+  }
+};
+// forward values: on-chip window, else recomputed
+struct FwdFetch {
+  const uint2* sm;
+  int ox, oy, w, m;
+  FwdEval eval;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
+    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    return eval(x, y);
+  }
+};
+// backward pass value at texel (x, y), as the advect_back texture would hold it
+struct BackEval {
+  SmemVel vel;
+  FwdFetch fwd;
+  float h;
+  int n, m;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+    const float2 p = texel_pos(x, y, m);
+    const float2 s = trace_pos(vel, p.x, p.y, -h, n);
+    return round_texel(bilerp(fwd, footprint(s.x, s.y, m)));
+  }
+};
+struct BackFetch {
+  const uint2* sm;
+  int ox, oy, w, m;
+  BackEval eval;
+  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
+    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    return eval(x, y);
+  }
+};
+
+__global__ void __launch_bounds__(kDyeThreads)
+    k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
+                const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
+                const DevSplats* __restrict__ S, int n, int m) {
+  extern __shared__ uint2 dsm[];
+  uint2* s_back = dsm;
+  uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
+  uint2* s_src = s_fwd + kDyeW2 * kDyeW2;
+  float2* s_vel = reinterpret_cast<float2*>(s_src + kDyeW3 * kDyeW3);
+  const int vw = dye_vel_edge(n, m);
+  const int tx0 = blockIdx.x * kDyeTile, ty0 = blockIdx.y * kDyeTile;
+  const int tid = threadIdx.x;
+  const float h = __fdiv_rn(dtbuf[0], kTwoPiF);
+
+  // origins (wrapped) of the on-chip windows
+  const int sx0 = (tx0 - 3 * kDyeHalo) & (m - 1), sy0 = (ty0 - 3 * kDyeHalo) & (m - 1);
+  const int fx0 = (tx0 - 2 * kDyeHalo) & (m - 1), fy0 = (ty0 - 2 * kDyeHalo) & (m - 1);
+  const int bx0 = (tx0 - kDyeHalo) & (m - 1), by0 = (ty0 - kDyeHalo) & (m - 1);
+  // velocity window: cells around the forward region, mapped to the n grid
+  const int vx0 = (int)floorf(((float)(tx0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
+
+  for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
+    const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
+    s_src[i] = __ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
+  }
+  for (int i = tid; i < vw * vw; i += kDyeThreads) {
+    const int ry = i / vw, rx = i - ry * vw;
+    s_vel[i] = __ldg(vel + (size_t)((vyw + ry) & (n - 1)) * n + ((vxw + rx) & (n - 1)));
+  }
+  __syncthreads();
+
+  const SmemVel V{s_vel, vxw, vyw, vw, n, vel};
+  const SmemTex T{s_src, sx0, sy0, kDyeW3, m, src};
+  const FwdEval fe{V, T, h, n, m};
+  for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
+    const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
+    const Rgba c = fe((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1));
+    s_fwd[i] = pack_texel(c.r, c.g, c.b, c.a);
+  }
+  __syncthreads();
+
+  const FwdFetch ff{s_fwd, fx0, fy0, kDyeW2, m, fe};
+  const BackEval be{V, ff, h, n, m};
+  for (int i = tid; i < kDyeW1 * kDyeW1; i += kDyeThreads) {
+    const int ry = i / kDyeW1, rx = i - ry * kDyeW1;
+    const Rgba c = be((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1));
+    s_back[i] = pack_texel(c.r, c.g, c.b, c.a);
+  }
+  __syncthreads();
+
+  const BackFetch bf{s_back, bx0, by0, kDyeW1, m, be};
+  const float fade = params->dye_fade;
+  for (int i = tid; i < kDyeTile * kDyeTile; i += kDyeThreads) {
+    const int ry = i / kDyeTile, rx = i - ry * kDyeTile;
+    const int x = tx0 + rx, y = ty0 + ry;
+    if (x >= m || y >= m) continue;
+    const float2 p = texel_pos(x, y, m);
+    const float2 s = trace_pos(V, p.x, p.y, h, n);
+    dst[(size_t)y * m + x] = correct_texel(T, bf, footprint(s.x, s.y, m), p.x, p.y, fade, S);
+  }
+}
+
+}  // namespace s2d

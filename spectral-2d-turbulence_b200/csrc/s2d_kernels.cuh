@@ -41,6 +41,9 @@ template <int N_> struct Tune {
   static constexpr int B_LDS = PL::stride(T >= 16 ? 0 : T);
   static constexpr int B_GRID = (N / 2) / PPB;
   static constexpr float KCUT = (float)(N / 3.0);
+  // resident CTAs the register budget must allow (128 registers a thread)
+  static constexpr int A_MINB = 65536 / (A_THREADS * 128) > 0 ? 65536 / (A_THREADS * 128) : 1;
+  static constexpr int B_MINB = 65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1;
   static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
   static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
   static constexpr size_t COLS_SMEM = sizeof(float2) * GA * A_LDS;
@@ -131,7 +134,7 @@ __device__ __forceinline__ float phys_cols_tile(const PhysArgs& a, int tile, flo
 }
 
 template <int N, int MODE>
-__global__ void __launch_bounds__(Tune<N>::A_THREADS) k_phys_cols(PhysArgs a) {
+__global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_cols(PhysArgs a) {
   using TU = Tune<N>;
   extern __shared__ float2 smem[];
   float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
@@ -279,7 +282,7 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
 }
 
 template <int N, int MODE, bool PTR>
-__global__ void __launch_bounds__(Tune<N>::B_THREADS) k_spec_rows(SpecArgs a) {
+__global__ void __launch_bounds__(Tune<N>::B_THREADS, Tune<N>::B_MINB) k_spec_rows(SpecArgs a) {
   extern __shared__ float2 smem[];
   spec_rows_tile<N, MODE, PTR>(a, blockIdx.x, smem);
 }

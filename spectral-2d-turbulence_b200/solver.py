@@ -267,6 +267,10 @@ class Solver:
     def encodeDye(self, pass_=None):
         L.call("s2d_encode_dye", self._use())
 
+    def encodeDyePasses(self, pass_=None):
+        """encodeDye as the reference's three dispatches (same bits as encodeDye)."""
+        L.call("s2d_encode_dye_passes", self._use())
+
     def encodeReduce(self, pass_=None):
         L.call("s2d_encode_reduce", self._use())
 

@@ -133,3 +133,29 @@ def test_dye_bfecc_step(pkg, m_scale):
         assert np.all(got[..., 3] == 1.0)
     finally:
         s.destroy()
+
+
+@pytest.mark.parametrize("n,m_scale", [(64, 1), (128, 2), (256, 4)])
+def test_fused_dye_equals_three_passes(pkg, n, m_scale):
+    """The one-launch dye step reproduces the reference's three dispatches bit for bit,
+    also when a large fixed dt pushes back-traces past the on-chip halo."""
+    splat = {"x": 0.1, "y": 0.9, "dx": -0.01, "dy": 0.02, "color": (0.36, 0.93, 0.66), "radius": 0.08,
+             "amp": 0.0, "dyeAmp": 1.0}
+    outs = []
+    for fused in (True, False):
+        s = pkg.Solver.create(n=n, dyeScale=m_scale)
+        try:
+            s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.02, dyeFade=0.99))
+            s.reset({"k0": 8, "amplitude": 10, "seed": 4, "dyePattern": "bands"})
+            s.setSplats([splat])
+            s.encodePrime()
+            for dt in (None, 0.05):                      # CFL dt, then a step of several texels
+                if dt is not None:
+                    set_fixed_dt(s, dt)
+                for _ in range(2):
+                    (s.encodeDye if fused else s.encodeDyePasses)()
+                outs.append(s.currentDye)
+        finally:
+            s.destroy()
+    assert np.array_equal(outs[0], outs[2])
+    assert np.array_equal(outs[1], outs[3])
