@@ -166,19 +166,27 @@ struct s2d_solver {
   int prof_cnt[S2D_PROF_CLASSES] = {0};
 };
 
-// RAII event pair around the launches of one kernel class (when profiling)
+// RAII event pair around the launches of one kernel class (when profiling).
+// Inside stream capture the records must be external to become event-record
+// nodes of the graph (a plain record there only orders the capture).
 struct ProfScope {
   s2d_solver* s;
   int cls;
   cudaEvent_t a = nullptr, b = nullptr;
+  static void record(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else cudaEventRecord(e, st);
+  }
   ProfScope(s2d_solver* s_, int c) : s(s_), cls(c) {
     if (!s->profiling) return;
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return;
-    cudaEventRecord(a, s->stream);
+    record(a, s->stream);
   }
   ~ProfScope() {
     if (!a || !b) return;
-    cudaEventRecord(b, s->stream);
+    record(b, s->stream);
     s->prof_events.emplace_back(cls, a, b);
   }
 };

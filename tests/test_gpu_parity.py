@@ -361,3 +361,21 @@ def test_seed_band_statistics(pkg):
         assert abs(np.std(phys.real) - 1.0) < 1e-5
     finally:
         s.destroy()
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_profiler_counts_every_kernel_class(pkg, graph):
+    s = pkg.Solver.create(n=128, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=2e-3))
+        s.reset({"k0": 14, "amplitude": 6, "seed": 1})
+        s.profile(True)
+        s.step(6, dye=True, reduce=True, graph=graph)
+        s.profileRead()
+        s.step(3, dye=True, reduce=True, graph=graph)
+        p = s.profileRead()
+        s.profile(False)
+        assert p["phys_cols"][1] == 9 and p["spec_rows"][1] == 9 and p["dye"][1] == 3
+        assert all(p[k][0] > 0 for k in ("phys_cols", "spec_rows", "dye"))
+    finally:
+        s.destroy()
