@@ -219,6 +219,27 @@ int s2d_profile(s2d_solver* s, int enable);
  * class since the last read, and clears them. */
 int s2d_profile_read(s2d_solver* s, double* ms /* S2D_PROF_CLASSES */, int* launches /* S2D_PROF_CLASSES */);
 
+/* ---------------------------------------------------------------- allocation-free CFL step */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- applications that reserve all GPU memory up front for their own
+ * allocator, or whose frame loop may not call cudaMalloc/cudaFree because those
+ * calls can synchronize the device -- this computes what s2d_encode_reduce
+ * computes, [dt, max |u|+|v|] with dt = clamp(cfl * (2 pi/n) / max, dt_min,
+ * dt_max) (dt_max when the maximum is <= 1e-8), from a caller-owned device
+ * velocity field `vel` (n*n interleaved (u, v) floats) into the caller-owned
+ * device buffer `dt_out` (2 floats), enqueued on `stream` (a cudaStream_t;
+ * NULL is the default stream), and allocates nothing.  Its only scratch is a
+ * static device array of S2D_CFL_STATIC_MAX_PARTIALS floats (16 KiB) that every
+ * GPU loading the library holds until the process exits, so n is limited to
+ * S2D_CFL_STATIC_MAX_N; larger n is rejected with S2D_ERR_ARG.  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress) with
+ * the device current; make that first call before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be ordered by the caller. */
+#define S2D_CFL_STATIC_MAX_N 4096
+#define S2D_CFL_STATIC_MAX_PARTIALS 4096
+int s2d_cfl_dt_static(const void* vel, int n, float cfl, float dt_min, float dt_max, void* dt_out, void* stream);
+
 /* ---------------------------------------------------------------- ensemble */
 /* Many independent instances of uneven sizes stepped together (no reference
  * counterpart beyond running many Solvers; BASELINE batching form). */
