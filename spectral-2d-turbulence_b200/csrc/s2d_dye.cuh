@@ -53,7 +53,7 @@ struct GlobalVel {
 // Every operation below is an explicitly rounded intrinsic (no multiply-add
 // contraction), so the fused and the three-pass kernels produce the same bits.
 __device__ __forceinline__ float lerp1(float a, float b, float t) {
-  return __fadd_rn(__fmul_rn(a, __fsub_rn(1.f, t)), __fmul_rn(b, t));   // WGSL mix(a, b, t)
+  return __fmaf_rn(b, t, __fmul_rn(a, __fsub_rn(1.f, t)));   // WGSL mix(a, b, t)
 }
 
 // bilinear velocity at normalised p (dye.wgsl:27-38); cell indices wrapped
@@ -75,14 +75,17 @@ __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - 
   return __fsub_rn(x, floorf(x));
 }
 
-// midpoint back-trace (dye.wgsl:40-45)
+// midpoint back-trace (dye.wgsl:40-45), from the velocity v1 already sampled at p
 template <class VF>
-__device__ __forceinline__ float2 trace_pos(const VF& vf, float px, float py, float h, int n) {
-  const float2 v1 = sample_vel(vf, px, py, n);
+__device__ __forceinline__ float2 trace_from(const VF& vf, float px, float py, float2 v1, float h, int n) {
   const float mx = fract_shift(px, __fmul_rn(0.5f, __fmul_rn(v1.x, h)));
   const float my = fract_shift(py, __fmul_rn(0.5f, __fmul_rn(v1.y, h)));
   const float2 v2 = sample_vel(vf, mx, my, n);
   return make_float2(fract_shift(px, __fmul_rn(v2.x, h)), fract_shift(py, __fmul_rn(v2.y, h)));
+}
+template <class VF>
+__device__ __forceinline__ float2 trace_pos(const VF& vf, float px, float py, float h, int n) {
+  return trace_from(vf, px, py, sample_vel(vf, px, py, n), h, n);
 }
 
 // texel footprint of a repeat-addressed linear sample at normalised s
@@ -128,13 +131,10 @@ __device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
   return make_float2(__fdiv_rn(__fadd_rn((float)x, 0.5f), mf), __fdiv_rn(__fadd_rn((float)y, 0.5f), mf));
 }
 
-// BFECC correction of one texel from its source and back-advected samples (dye.wgsl:81-112)
-template <class SF, class BF>
-__device__ __forceinline__ uint2 correct_texel(const SF& src, const BF& back, const Footprint& f, float px, float py,
-                                               float fade, const DevSplats* __restrict__ S) {
-  Rgba lo, hi;
-  const Rgba a = bilerp(src, f, &lo, &hi);
-  const Rgba b = bilerp(back, f);
+// BFECC correction of one texel from its source (a, with the 4-texel min/max) and
+// back-advected (b) samples, fade and splat dye (dye.wgsl:81-112)
+__device__ __forceinline__ uint2 correct_from(const Rgba& a, const Rgba& b, const Rgba& lo, const Rgba& hi, float px,
+                                              float py, float fade, const DevSplats* __restrict__ S) {
   auto corr = [&](float x, float y, float l, float u) {
     return __fmul_rn(fminf(fmaxf(__fsub_rn(__fmul_rn(1.5f, x), __fmul_rn(0.5f, y)), l), u), fade);
   };
@@ -155,6 +155,15 @@ __device__ __forceinline__ uint2 correct_texel(const SF& src, const BF& back, co
     }
   }
   return pack_texel(r, g, bb, 1.f);
+}
+
+template <class SF, class BF>
+__device__ __forceinline__ uint2 correct_texel(const SF& src, const BF& back, const Footprint& f, float px, float py,
+                                               float fade, const DevSplats* __restrict__ S) {
+  Rgba lo, hi;
+  const Rgba a = bilerp(src, f, &lo, &hi);
+  const Rgba b = bilerp(back, f);
+  return correct_from(a, b, lo, hi, px, py, fade, S);
 }
 
 // ---------------------------------------------------------------- three passes (reference order)
@@ -195,19 +204,34 @@ constexpr int kDyeW3 = kDyeTile + 6 * kDyeHalo;   // source region edge
 // under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
 __host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
 __host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
-  return sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
-         sizeof(float2) * dye_vel_edge(n, m) * dye_vel_edge(n, m);
+  return sizeof(float4) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
+         sizeof(float2) * (2 * kDyeW2 * kDyeW2 + dye_vel_edge(n, m) * dye_vel_edge(n, m));
 }
 
-// on-chip window with an exact global fallback; coordinates are wrapped grid indices
+__device__ __forceinline__ Rgba from4(float4 v) { return {v.x, v.y, v.z, v.w}; }
+
+// on-chip window of FP32 texels with an exact global fallback (coordinates are wrapped indices)
 struct SmemTex {
-  const uint2* sm;
+  const float4* sm;
   int ox, oy, w, m;
   const uint2* g;
   __device__ __forceinline__ Rgba operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
     return unpack_texel(__ldg(g + (size_t)y * m + x));
+  }
+  // the 2x2 footprint in one window test (slots rx, rx+1 hold texels x0, x1 = x0+1 wrapped)
+  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
+    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
+    if (rx + 1 < w && ry + 1 < w) {
+      const float4* p = sm + ry * w + rx;
+      c00 = from4(p[0]);
+      c10 = from4(p[1]);
+      c01 = from4(p[w]);
+      c11 = from4(p[w + 1]);
+      return true;
+    }
+    return false;
   }
 };
 struct SmemVel {
@@ -221,61 +245,143 @@ struct SmemVel {
   }
 };
 
-// forward pass value at texel (x, y), as the advect_fwd texture would hold it
+// bilinear velocity with one window test for the 2x2 cell footprint (same arithmetic as sample_vel)
+__device__ __forceinline__ float2 sample_vel_win(const SmemVel& vf, float px, float py) {
+  const int n = vf.n;
+  const float nf = (float)n;
+  const float gx = __fsub_rn(__fmul_rn(px, nf), 0.5f), gy = __fsub_rn(__fmul_rn(py, nf), 0.5f);
+  const float bx = floorf(gx), by = floorf(gy);
+  const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
+  const int ix = (int)bx, iy = (int)by;
+  const int rx = (ix - vf.ox) & (n - 1), ry = (iy - vf.oy) & (n - 1);
+  float2 v00, v10, v01, v11;
+  if (rx + 1 < vf.w && ry + 1 < vf.w) {
+    const float2* p = vf.sm + ry * vf.w + rx;
+    v00 = p[0];
+    v10 = p[1];
+    v01 = p[vf.w];
+    v11 = p[vf.w + 1];
+  } else {
+    const int x0 = ix & (n - 1), x1 = (ix + 1) & (n - 1), y0 = iy & (n - 1), y1 = (iy + 1) & (n - 1);
+    v00 = vf(x0, y0);
+    v10 = vf(x1, y0);
+    v01 = vf(x0, y1);
+    v11 = vf(x1, y1);
+  }
+  return make_float2(lerp1(lerp1(v00.x, v10.x, fx), lerp1(v01.x, v11.x, fx), fy),
+                     lerp1(lerp1(v00.y, v10.y, fx), lerp1(v01.y, v11.y, fx), fy));
+}
+struct WinVel {      // adapter: the window sampler where trace_from expects sample_vel
+  const SmemVel& v;
+};
+__device__ __forceinline__ float2 sample_vel(const WinVel& w, float px, float py, int) {
+  return sample_vel_win(w.v, px, py);
+}
+
+template <class TF>
+__device__ __forceinline__ Rgba bilerp_win(const TF& tf, const Footprint& f, Rgba* lo = nullptr, Rgba* hi = nullptr) {
+  Rgba c00, c10, c01, c11;
+  if (!tf.quad(f, c00, c10, c01, c11)) {
+    c00 = tf(f.x0, f.y0);
+    c10 = tf(f.x1, f.y0);
+    c01 = tf(f.x0, f.y1);
+    c11 = tf(f.x1, f.y1);
+  }
+  if (lo) {
+    lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
+    lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
+    lo->b = fminf(fminf(c00.b, c10.b), fminf(c01.b, c11.b));
+    hi->r = fmaxf(fmaxf(c00.r, c10.r), fmaxf(c01.r, c11.r));
+    hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
+    hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
+  }
+  return {lerp2(c00.r, c10.r, c01.r, c11.r, f.fx, f.fy), lerp2(c00.g, c10.g, c01.g, c11.g, f.fx, f.fy),
+          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
+}
+
+// forward-pass value at texel (x, y), as the advect_fwd texture would hold it
 struct FwdEval {
-  SmemVel vel;
-  SmemTex src;
+  const SmemVel& vel;
+  const SmemTex& src;
   float h;
   int n, m;
   __device__ __forceinline__ Rgba operator()(int x, int y) const {
     const float2 p = texel_pos(x, y, m);
-    const float2 s = trace_pos(vel, p.x, p.y, h, n);
-    return round_texel(bilerp(src, footprint(s.x, s.y, m)));
+    const float2 s = trace_from(WinVel{vel}, p.x, p.y, sample_vel_win(vel, p.x, p.y), h, n);
+    return round_texel(bilerp_win(src, footprint(s.x, s.y, m)));
   }
 };
 // forward values: on-chip window, else recomputed
 struct FwdFetch {
-  const uint2* sm;
+  const float4* sm;
   int ox, oy, w, m;
-  FwdEval eval;
+  const FwdEval& eval;
   __device__ __forceinline__ Rgba operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
     return eval(x, y);
   }
+  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
+    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
+    if (rx + 1 < w && ry + 1 < w) {
+      const float4* p = sm + ry * w + rx;
+      c00 = from4(p[0]);
+      c10 = from4(p[1]);
+      c01 = from4(p[w]);
+      c11 = from4(p[w + 1]);
+      return true;
+    }
+    return false;
+  }
 };
-// backward pass value at texel (x, y), as the advect_back texture would hold it
+// backward-pass value at texel (x, y), as the advect_back texture would hold it
 struct BackEval {
-  SmemVel vel;
-  FwdFetch fwd;
+  const SmemVel& vel;
+  const FwdFetch& fwd;
   float h;
   int n, m;
   __device__ __forceinline__ Rgba operator()(int x, int y) const {
     const float2 p = texel_pos(x, y, m);
-    const float2 s = trace_pos(vel, p.x, p.y, -h, n);
-    return round_texel(bilerp(fwd, footprint(s.x, s.y, m)));
+    const float2 s = trace_from(WinVel{vel}, p.x, p.y, sample_vel_win(vel, p.x, p.y), -h, n);
+    return round_texel(bilerp_win(fwd, footprint(s.x, s.y, m)));
   }
 };
 struct BackFetch {
-  const uint2* sm;
+  const float4* sm;
   int ox, oy, w, m;
-  BackEval eval;
+  const BackEval& eval;
   __device__ __forceinline__ Rgba operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return unpack_texel(sm[ry * w + rx]);
+    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
     return eval(x, y);
   }
+  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
+    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
+    if (rx + 1 < w && ry + 1 < w) {
+      const float4* p = sm + ry * w + rx;
+      c00 = from4(p[0]);
+      c10 = from4(p[1]);
+      c01 = from4(p[w]);
+      c11 = from4(p[w + 1]);
+      return true;
+    }
+    return false;
+  }
 };
+
+__device__ __forceinline__ float4 to4(const Rgba& c) { return make_float4(c.r, c.g, c.b, c.a); }
 
 __global__ void __launch_bounds__(kDyeThreads)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
                 const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
                 const DevSplats* __restrict__ S, int n, int m) {
-  extern __shared__ uint2 dsm[];
-  uint2* s_back = dsm;
-  uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
-  uint2* s_src = s_fwd + kDyeW2 * kDyeW2;
-  float2* s_vel = reinterpret_cast<float2*>(s_src + kDyeW3 * kDyeW3);
+  extern __shared__ float4 dsm4[];
+  float4* s_back = dsm4;
+  float4* s_fwd = s_back + kDyeW1 * kDyeW1;
+  float4* s_src = s_fwd + kDyeW2 * kDyeW2;
+  float2* s_v1 = reinterpret_cast<float2*>(s_src + kDyeW3 * kDyeW3);   // velocity at forward-region texels
+  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // forward trace positions
+  float2* s_vel = s_sp + kDyeW2 * kDyeW2;
   const int vw = dye_vel_edge(n, m);
   const int tx0 = blockIdx.x * kDyeTile, ty0 = blockIdx.y * kDyeTile;
   const int tid = threadIdx.x;
@@ -285,14 +391,13 @@ __global__ void __launch_bounds__(kDyeThreads)
   const int sx0 = (tx0 - 3 * kDyeHalo) & (m - 1), sy0 = (ty0 - 3 * kDyeHalo) & (m - 1);
   const int fx0 = (tx0 - 2 * kDyeHalo) & (m - 1), fy0 = (ty0 - 2 * kDyeHalo) & (m - 1);
   const int bx0 = (tx0 - kDyeHalo) & (m - 1), by0 = (ty0 - kDyeHalo) & (m - 1);
-  // velocity window: cells around the forward region, mapped to the n grid
   const int vx0 = (int)floorf(((float)(tx0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
 
   for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
     const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
-    s_src[i] = __ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
+    s_src[i] = to4(unpack_texel(__ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)))));
   }
   for (int i = tid; i < vw * vw; i += kDyeThreads) {
     const int ry = i / vw, rx = i - ry * vw;
@@ -302,32 +407,49 @@ __global__ void __launch_bounds__(kDyeThreads)
 
   const SmemVel V{s_vel, vxw, vyw, vw, n, vel};
   const SmemTex T{s_src, sx0, sy0, kDyeW3, m, src};
-  const FwdEval fe{V, T, h, n, m};
+  // velocity at every forward-region texel centre: shared by the +h and -h traces
   for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
     const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
-    const Rgba c = fe((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1));
-    s_fwd[i] = pack_texel(c.r, c.g, c.b, c.a);
+    const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
+    s_v1[i] = sample_vel_win(V, p.x, p.y);
   }
   __syncthreads();
 
+  // forward pass over the forward region; keep its trace positions for the correction
+  for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
+    const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
+    const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
+    const float2 sp = trace_from(WinVel{V}, p.x, p.y, s_v1[i], h, n);
+    s_sp[i] = sp;
+    s_fwd[i] = to4(round_texel(bilerp_win(T, footprint(sp.x, sp.y, m))));
+  }
+  __syncthreads();
+
+  const FwdEval fe{V, T, h, n, m};
   const FwdFetch ff{s_fwd, fx0, fy0, kDyeW2, m, fe};
-  const BackEval be{V, ff, h, n, m};
+  // backward pass over the backward region (nested in the forward region by kDyeHalo)
   for (int i = tid; i < kDyeW1 * kDyeW1; i += kDyeThreads) {
     const int ry = i / kDyeW1, rx = i - ry * kDyeW1;
-    const Rgba c = be((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1));
-    s_back[i] = pack_texel(c.r, c.g, c.b, c.a);
+    const int fi = (ry + kDyeHalo) * kDyeW2 + rx + kDyeHalo;
+    const float2 p = texel_pos((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1), m);
+    const float2 sb = trace_from(WinVel{V}, p.x, p.y, s_v1[fi], -h, n);
+    s_back[i] = to4(round_texel(bilerp_win(ff, footprint(sb.x, sb.y, m))));
   }
   __syncthreads();
 
+  const BackEval be{V, ff, h, n, m};
   const BackFetch bf{s_back, bx0, by0, kDyeW1, m, be};
   const float fade = params->dye_fade;
   for (int i = tid; i < kDyeTile * kDyeTile; i += kDyeThreads) {
     const int ry = i / kDyeTile, rx = i - ry * kDyeTile;
     const int x = tx0 + rx, y = ty0 + ry;
-    if (x >= m || y >= m) continue;
     const float2 p = texel_pos(x, y, m);
-    const float2 s = trace_pos(V, p.x, p.y, h, n);
-    dst[(size_t)y * m + x] = correct_texel(T, bf, footprint(s.x, s.y, m), p.x, p.y, fade, S);
+    const float2 sp = s_sp[(ry + 2 * kDyeHalo) * kDyeW2 + rx + 2 * kDyeHalo];
+    const Footprint f = footprint(sp.x, sp.y, m);
+    Rgba lo, hi;
+    const Rgba a = bilerp_win(T, f, &lo, &hi);
+    const Rgba b = bilerp_win(bf, f);
+    dst[(size_t)y * m + x] = correct_from(a, b, lo, hi, p.x, p.y, fade, S);
   }
 }
 

@@ -197,18 +197,22 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
   const bool row_band = fabsf(ky) < KCUT;
   const size_t rbase = (size_t)row * N;
 
-  float2 nh[V];
+  // own0: the exchange line of this row's transforms; own1: this row's N_hat, then
+  // its updated state, in natural (padded) order -- each thread touches only the
+  // slots of its own elements there, so own1 needs no barrier.
+  using PL = LinePlan<N, V>;
+  bool any_band = false;
   if constexpr (MODE >= 0) {
     // the first pair of this CTA has the smallest |ky|: the CTA is uniformly in/out of band work
-    const bool cta_band = (float)(tile * TU::PPB) < KCUT;
-    if (cta_band) {
+    any_band = (float)(tile * TU::PPB) < KCUT;
+    if (any_band) {
       float2 zz[1][V];
 #pragma unroll
       for (int m = 0; m < V; ++m) zz[0][m] = row_band ? __ldcs(a.z + rbase + t + T * m) : make_float2(0.f, 0.f);
       float2* const zb[1] = {own0};
       fft_lines<N, V, -1, 1>(zz, zb, t, a.tw, CtaSync{});
 #pragma unroll
-      for (int m = 0; m < V; ++m) own0[LinePlan<N, V>::pad(t + T * m)] = zz[0][m];
+      for (int m = 0; m < V; ++m) own0[PL::pad(t + T * m)] = zz[0][m];
       __syncthreads();
       const float2* pbuf = smem + (2 * pslot) * LDS;
 #pragma unroll
@@ -216,68 +220,78 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
         const int c = t + T * m;
         const float kx = wn<N>(c);
         const float2 zk = zz[0][m];
-        const float2 zm = cconj(pbuf[LinePlan<N, V>::pad((N - c) & (N - 1))]);
+        const float2 zm = cconj(pbuf[PL::pad((N - c) & (N - 1))]);
         // q1 = (Z_k + conj Z_-k)/2, q2 = -i (Z_k - conj Z_-k)/2 (solver.wgsl:68-72)
         const float2 q1 = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
         const float2 dd = csub(zk, zm);
         const float2 q2 = make_float2(0.5f * dd.y, -0.5f * dd.x);
         const bool band = row_band && fabsf(kx) < KCUT;
         // N_hat = kx * (i q1) + ky * (i q2)
-        nh[m] = band ? make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x) : make_float2(0.f, 0.f);
+        own1[PL::pad(c)] =
+            band ? make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x) : make_float2(0.f, 0.f);
       }
-      __syncthreads();
-    } else {
-#pragma unroll
-      for (int m = 0; m < V; ++m) nh[m] = make_float2(0.f, 0.f);
+      __syncthreads();   // partner reads of own0 done before the transforms below reuse it
     }
   }
 
-  float2 p[2][V];
+  // RK3 stage update, one cell per iteration (kept rolled: the forcing and
+  // integrating-factor code appears once in the kernel, not 16 times)
   {
     const DevParams& P = *a.params;
     float dt = 0.f;
     if constexpr (MODE >= 0) dt = __ldg(a.dt);
-    constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
-#pragma unroll
+#pragma unroll 1
     for (int m = 0; m < V; ++m) {
       const int c = t + T * m;
       const size_t o = rbase + c;
-      const float kx = wn<N>(c);
-      const float k2 = kx * kx + ky * ky;
       float2 w;
       if constexpr (MODE < 0) {
         w = a.wcur[o];
       } else {
+        const float kx = wn<N>(c);
+        const float k2 = kx * kx + ky * ky;
         const float2 wc = a.wcur[o];
         const float2 w0 = MODE == 0 ? wc : a.w0[o];
         const bool band = row_band && fabsf(kx) < KCUT;
-        float2 rhs = make_float2(-nh[m].x, -nh[m].y);
+        const float2 nhat = any_band ? own1[PL::pad(c)] : make_float2(0.f, 0.f);
+        float2 rhs = make_float2(-nhat.x, -nhat.y);
         if constexpr (PTR) {
           if (band) rhs = cadd(rhs, __ldg(a.fptr + o));
         }
         if (a.stochastic && band && k2 > 0.f) rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
-        if (k2 == 0.f) {
-          w = make_float2(0.f, 0.f);
-        } else {
-          w = rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
-        }
+        w = k2 == 0.f ? make_float2(0.f, 0.f) : rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
         a.wout[o] = w;
       }
-      // next-stage packs, scaled by the 1/N^2 of the inverse 2D transform
-      const float inv = k2 > 0.f ? 1.f / k2 : 0.f;
-      const float fa = (1.f - ky * inv) * inv_n2;     // w + i u_hat = w (1 - ky/k2)
-      const float fb = kx * inv * inv_n2;              // v_hat = -i kx w / k2
-      p[0][m] = make_float2(w.x * fa, w.y * fa);
-      p[1][m] = make_float2(w.y * fb, -w.x * fb);
+      own1[PL::pad(c)] = w;
     }
   }
-  float2* const pbufs[2] = {own0, own1};
-  fft_lines<N, V, +1, 2>(p, pbufs, t, a.tw, CtaSync{});
+
+  // next-stage packs, scaled by the 1/N^2 of the inverse 2D transform, x-IFFT each;
+  // the two transforms share one code path
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+#pragma unroll 1
+  for (int q = 0; q < 2; ++q) {
+    float2 x[1][V];
 #pragma unroll
-  for (int m = 0; m < V; ++m) {
-    const size_t o = rbase + t + T * m;
-    a.pa[o] = p[0][m];
-    a.pb[o] = p[1][m];
+    for (int m = 0; m < V; ++m) {
+      const int c = t + T * m;
+      const float kx = wn<N>(c);
+      const float k2 = kx * kx + ky * ky;
+      const float inv = k2 > 0.f ? __frcp_rn(k2) : 0.f;
+      const float2 w = own1[PL::pad(c)];
+      if (q == 0) {
+        const float fa = (1.f - ky * inv) * inv_n2;     // w + i u_hat = w (1 - ky/k2)
+        x[0][m] = make_float2(w.x * fa, w.y * fa);
+      } else {
+        const float fb = kx * inv * inv_n2;              // v_hat = -i kx w / k2
+        x[0][m] = make_float2(w.y * fb, -w.x * fb);
+      }
+    }
+    float2* const xb[1] = {own0};
+    fft_lines<N, V, +1, 1>(x, xb, t, a.tw, CtaSync{});
+    float2* const dst = q == 0 ? a.pa : a.pb;
+#pragma unroll
+    for (int m = 0; m < V; ++m) dst[rbase + t + T * m] = x[0][m];
   }
 }
 
