@@ -142,6 +142,7 @@ struct s2d_solver {
   float* zonal = nullptr;
   double* seed_parts = nullptr;
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
+  int* err = nullptr;                 // device error word (bounded waits that gave up)
   ushort4* dye[3] = {nullptr, nullptr, nullptr};
   // pinned readback staging (copyDiagnostics)
   double* h_diag = nullptr;
@@ -210,7 +211,7 @@ static void free_solver(s2d_solver* s) {
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
                       s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->dye[0], s->dye[1], s->dye[2]};
+                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
   void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
@@ -372,6 +373,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMalloc(&s->zonal, sizeof(float) * n), "zonal");
   TRY(cudaMalloc(&s->seed_parts, sizeof(double) * seed_parts_count(n)), "seed partials");
   TRY(cudaMalloc(&s->step_counter, sizeof(uint32_t)), "step counter");
+  TRY(cudaMalloc(&s->err, sizeof(int)), "error word");
+  TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream), "memset");
   TRY(cudaMemsetAsync(s->step_counter, 0, sizeof(uint32_t), s->stream), "memset");
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
   TRY(cudaMallocHost(&s->h_diag, sizeof(double) * (s->nbins + 2)), "pinned diag");
@@ -458,11 +461,23 @@ extern "C" int s2d_get_stream(s2d_solver* s, void** stream) {
   return S2D_OK;
 }
 
+// reports (and clears) a bounded device-side wait that gave up since the last check
+static int check_device_error(s2d_solver* s) {
+  int h = 0;
+  S2D_CUDA(cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  if (h) {
+    cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+    return fail(S2D_ERR_CUDA, "a device-side wait for staged rows timed out; results of that step are invalid");
+  }
+  return S2D_OK;
+}
+
 extern "C" int s2d_synchronize(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
   S2D_CUDA(cudaStreamSynchronize(s->stream));
-  return S2D_OK;
+  return check_device_error(s);
 }
 
 // ------------------------------------------------------------------ parameters
@@ -534,6 +549,7 @@ static int enqueue_pack_prime(s2d_solver* s) {
   a.dt = dt_slot(s, s->slot);
   a.params = s->dparams;
   a.tw = s->tw;
+  a.err = s->err;
   s->ops->spec_rows(-1, false, a, s->stream);
   S2D_LAUNCHED();
   s->packs_valid = true;
@@ -603,6 +619,7 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     a.params = s->dparams;
     a.tw = s->tw;
     a.stochastic = s->hp.force_amp > 0.f ? 1 : 0;
+    a.err = s->err;
     s->ops->spec_rows(st, ptr, a, s->stream);
     S2D_LAUNCHED();
   }
@@ -977,8 +994,7 @@ extern "C" int s2d_get_buffer(s2d_solver* s, int id, void* host, size_t bytes) {
   }
   if (bytes > sz) return fail(S2D_ERR_ARG, "requested more bytes than the buffer holds");
   S2D_CUDA(cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, s->stream));
-  S2D_CUDA(cudaStreamSynchronize(s->stream));
-  return S2D_OK;
+  return check_device_error(s);
 }
 
 extern "C" int s2d_set_buffer(s2d_solver* s, int id, const void* host, size_t bytes) {

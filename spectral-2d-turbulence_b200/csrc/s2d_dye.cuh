@@ -126,9 +126,11 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
           lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
 }
 
+// texel centre (x + 0.5)/m; m is a power of two, so the product with 1/m is the
+// exactly rounded quotient
 __device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
-  const float mf = (float)m;
-  return make_float2(__fdiv_rn(__fadd_rn((float)x, 0.5f), mf), __fdiv_rn(__fadd_rn((float)y, 0.5f), mf));
+  const float inv = __frcp_rn((float)m);
+  return make_float2(__fmul_rn(__fadd_rn((float)x, 0.5f), inv), __fmul_rn(__fadd_rn((float)y, 0.5f), inv));
 }
 
 // BFECC correction of one texel from its source (a, with the 4-texel min/max) and
@@ -395,10 +397,12 @@ __global__ void __launch_bounds__(kDyeThreads)
   const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
 
+#pragma unroll 4
   for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
     const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
     s_src[i] = to4(unpack_texel(__ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)))));
   }
+#pragma unroll 4
   for (int i = tid; i < vw * vw; i += kDyeThreads) {
     const int ry = i / vw, rx = i - ry * vw;
     s_vel[i] = __ldg(vel + (size_t)((vyw + ry) & (n - 1)) * n + ((vxw + rx) & (n - 1)));

@@ -61,9 +61,15 @@ constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
 constexpr size_t kEnsASmem =
     cmax(cmax(cmax(Tune<64>::A_SMEM, Tune<128>::A_SMEM), cmax(Tune<256>::A_SMEM, Tune<512>::A_SMEM)),
          Tune<1024>::A_SMEM);
-constexpr size_t kEnsBSmem =
+// one layout for every size: exchange lines, staged rows, then the barrier
+constexpr size_t kEnsBStageOff =
     cmax(cmax(cmax(Tune<64>::B_SMEM, Tune<128>::B_SMEM), cmax(Tune<256>::B_SMEM, Tune<512>::B_SMEM)),
          Tune<1024>::B_SMEM);
+constexpr size_t kEnsBStageBytes =
+    cmax(cmax(cmax(Tune<64>::B_STAGE_BYTES, Tune<128>::B_STAGE_BYTES),
+              cmax(Tune<256>::B_STAGE_BYTES, Tune<512>::B_STAGE_BYTES)),
+         Tune<1024>::B_STAGE_BYTES);
+constexpr size_t kEnsBSmem = kEnsBStageOff + kEnsBStageBytes + 16;
 
 struct Pools {
   float2* s[3];
@@ -93,12 +99,27 @@ __global__ void __launch_bounds__(kEnsAThreads, 2)
   }
 }
 
+// the per-size tile functions place staged rows and the barrier at Tune<N> offsets;
+// the ensemble kernel hands each size a window whose offsets match by shifting the
+// base pointer so that Tune<N>::B_STAGE_OFF lands on the common staging offset
+template <int N> __device__ __forceinline__ float2* ens_spec_base(float2* smem) {
+  return reinterpret_cast<float2*>(reinterpret_cast<char*>(smem) + (kEnsBStageOff - Tune<N>::B_STAGE_OFF));
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kEnsBThreads, 4)
-    k_ens_spec(const EnsInst* __restrict__ inst, const int2* __restrict__ items, int nitems, Pools pool, int phase) {
-  extern __shared__ float2 smem[];
+    k_ens_spec(const EnsInst* __restrict__ inst, const int2* __restrict__ items, int nitems, Pools pool, int phase,
+               int* err) {
+  extern __shared__ __align__(16) float2 smem[];
   const int st = MODE < 0 ? 0 : MODE;
-  for (int k = blockIdx.x; k < nitems; k += gridDim.x) {
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + kEnsBStageOff + kEnsBStageBytes);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  for (int k = blockIdx.x; k < nitems; k += gridDim.x, parity ^= 1u) {
     const int2 it = items[k];
     const EnsInst& I = inst[it.x];
     SpecArgs a{};
@@ -112,12 +133,13 @@ __global__ void __launch_bounds__(kEnsBThreads, 4)
     a.params = &I.p;
     a.tw = I.tw;
     a.stochastic = I.p.force_amp > 0.f ? 1 : 0;
+    a.err = err;
     switch (I.n) {
-      case 64: spec_rows_tile<64, MODE, false>(a, it.y, smem); break;
-      case 128: spec_rows_tile<128, MODE, false>(a, it.y, smem); break;
-      case 256: spec_rows_tile<256, MODE, false>(a, it.y, smem); break;
-      case 512: spec_rows_tile<512, MODE, false>(a, it.y, smem); break;
-      default: spec_rows_tile<1024, MODE, false>(a, it.y, smem); break;
+      case 64: spec_rows_tile<64, MODE, false>(a, it.y, ens_spec_base<64>(smem), bar, parity); break;
+      case 128: spec_rows_tile<128, MODE, false>(a, it.y, ens_spec_base<128>(smem), bar, parity); break;
+      case 256: spec_rows_tile<256, MODE, false>(a, it.y, ens_spec_base<256>(smem), bar, parity); break;
+      case 512: spec_rows_tile<512, MODE, false>(a, it.y, ens_spec_base<512>(smem), bar, parity); break;
+      default: spec_rows_tile<1024, MODE, false>(a, it.y, ens_spec_base<1024>(smem), bar, parity); break;
     }
     __syncthreads();
   }
@@ -202,6 +224,7 @@ struct s2d_ensemble {
   Pools pool{};
   float2* tw = nullptr;
   double* sums = nullptr;    // 2 * count
+  int* err = nullptr;        // device error word (bounded waits that gave up)
   long long cells = 0;
   int phase = 0;
   bool packs_valid = false;
@@ -214,7 +237,7 @@ static void ens_free(s2d_ensemble* e) {
     if (kv.second.first) cudaGraphDestroy(kv.second.first);
   }
   void* ptrs[] = {e->dinst, e->dseeds, e->items_a, e->items_b, e->pool.s[0], e->pool.s[1], e->pool.s[2],
-                  e->pool.pa, e->pool.pb, e->pool.z, e->tw, e->sums};
+                  e->pool.pa, e->pool.pb, e->pool.z, e->tw, e->sums, e->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -317,6 +340,8 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
   TRY(cudaMalloc(&e->items_a, sizeof(int2) * ia.size()), "items");
   TRY(cudaMalloc(&e->items_b, sizeof(int2) * ib.size()), "items");
   TRY(cudaMalloc(&e->sums, sizeof(double) * 2 * count), "sums");
+  TRY(cudaMalloc(&e->err, sizeof(int)), "error word");
+  TRY(cudaMemsetAsync(e->err, 0, sizeof(int), e->stream), "memset");
   const size_t cbytes = sizeof(float2) * (size_t)off;
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&e->pool.s[i], cbytes), "state pool");
   TRY(cudaMalloc(&e->pool.pa, cbytes), "pack pool");
@@ -364,10 +389,20 @@ extern "C" int s2d_ensemble_get_stream(s2d_ensemble* e, void** stream) {
   return S2D_OK;
 }
 
+static int ens_check_err(s2d_ensemble* e) {
+  int h = 0;
+  E_CUDA(cudaMemcpy(&h, e->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    cudaMemset(e->err, 0, sizeof(int));
+    return efail(S2D_ERR_CUDA, "a device-side wait for staged rows timed out; results of that step are invalid");
+  }
+  return S2D_OK;
+}
+
 extern "C" int s2d_ensemble_synchronize(s2d_ensemble* e) {
   E_USE(e);
   E_CUDA(cudaStreamSynchronize(e->stream));
-  return S2D_OK;
+  return ens_check_err(e);
 }
 
 extern "C" int s2d_ensemble_seed_band(s2d_ensemble* e, float kmin, float kmax, float rms) {
@@ -407,7 +442,7 @@ extern "C" int s2d_ensemble_get_state(s2d_ensemble* e, int index, float* spectru
   E_CUDA(cudaMemcpyAsync(spectrum, e->pool.s[e->phase] + I.off, sizeof(float2) * (size_t)I.n * I.n,
                          cudaMemcpyDeviceToHost, e->stream));
   E_CUDA(cudaStreamSynchronize(e->stream));
-  return S2D_OK;
+  return ens_check_err(e);
 }
 
 static int ens_enqueue_step(s2d_ensemble* e) {
@@ -415,9 +450,9 @@ static int ens_enqueue_step(s2d_ensemble* e) {
   for (int st = 0; st < 3; ++st) {
     k_ens_phys<<<e->grid_a, kEnsAThreads, kEnsASmem, e->stream>>>(e->dinst, e->items_a, e->nitems_a, e->pool);
     E_LAUNCHED();
-    if (st == 0) k_ens_spec<0><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p);
-    else if (st == 1) k_ens_spec<1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p);
-    else k_ens_spec<2><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p);
+    if (st == 0) k_ens_spec<0><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
+    else if (st == 1) k_ens_spec<1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
+    else k_ens_spec<2><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
     E_LAUNCHED();
   }
   e->phase = (p + 1) % 3;
@@ -432,7 +467,7 @@ extern "C" int s2d_ensemble_step(s2d_ensemble* e, int steps, int use_graph) {
   if (prev != e->dev) cudaSetDevice(e->dev);
   int rc = S2D_OK;
   if (!e->packs_valid) {
-    k_ens_spec<-1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, e->phase);
+    k_ens_spec<-1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, e->phase, e->err);
     if (cudaGetLastError() != cudaSuccess) rc = efail(S2D_ERR_CUDA, "prime launch failed");
     e->packs_valid = true;
   }

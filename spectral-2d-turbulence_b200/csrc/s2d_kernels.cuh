@@ -20,6 +20,7 @@
 // (velocity_pack, nl_pack, assemble, rk3, fft rows/cols) reproduce the
 // reference's unfused stages one for one, for the per-stage test hooks.
 #pragma once
+#include "s2d_async.cuh"
 #include "s2d_device.cuh"
 
 namespace s2d {
@@ -46,6 +47,13 @@ template <int N_> struct Tune {
   static constexpr int B_MINB = 65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1;
   static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
   static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
+  // rows the spectral-row kernel stages by TMA bulk copy (wcur, w0, pointer force),
+  // after the exchange lines; off at N = 4096, where they would not fit
+  static constexpr bool PREFETCH = N <= 2048;
+  static constexpr size_t B_STAGE_OFF = B_SMEM;
+  static constexpr size_t B_STAGE_BYTES = PREFETCH ? sizeof(float2) * 3 * B_ROWS * N : 0;
+  static constexpr size_t B_BAR_OFF = B_STAGE_OFF + B_STAGE_BYTES;
+  static constexpr size_t B_SMEM_TOTAL = B_BAR_OFF + 16;
   static constexpr size_t COLS_SMEM = sizeof(float2) * GA * A_LDS;
   static constexpr size_t ROWS_SMEM = sizeof(float2) * B_ROWS * B_LDS;
 };
@@ -81,7 +89,20 @@ struct SpecArgs {
   const DevParams* params;
   const float2* tw;
   int stochastic;       // force_amp > 0
+  int* err;             // device error word (bounded waits that gave up)
 };
+
+// rows held by the 2*PPB row slots of tile `tile`: pair p = rows (p, N-p); pair 0 = rows (0, N/2)
+template <int N> __device__ __forceinline__ int spec_row_of(int tile, int slot) {
+  const int pair = tile * Tune<N>::PPB + (slot >> 1);
+  const int which = slot & 1;
+  return pair == 0 ? (which ? N / 2 : 0) : (which ? N - pair : pair);
+}
+
+// number of staged row arrays for a stage: wcur, w0 (stages 1-2), pointer force
+template <int MODE, bool PTR> __host__ __device__ constexpr int spec_stage_arrays() {
+  return (MODE >= 1 ? 2 : 1) + (PTR ? 1 : 0);
+}
 
 // ---------------------------------------------------------------------------------------
 // physical columns: MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage
@@ -180,17 +201,38 @@ __global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_co
 
 // ---------------------------------------------------------------------------------------
 // spectral row pairs: MODE -1 = prime (pack wcur only), 0/1/2 = RK stage
+// `bar` is an initialised mbarrier in shared memory whose next phase is `parity`
+// (one phase per call); it orders the TMA bulk copies of this tile's rows.
 template <int N, int MODE, bool PTR>
-__device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, float2* smem) {
+__device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, float2* smem, uint64_t* bar,
+                                               uint32_t parity) {
   using TU = Tune<N>;
   constexpr int V = TU::V, T = TU::T, LDS = TU::B_LDS;
   constexpr float KCUT = TU::KCUT;
+  constexpr int NARR = spec_stage_arrays<MODE, PTR>();
   const int tid = threadIdx.x;
   const int t = tid % T, slot = tid / T;
   const int pair = tile * TU::PPB + (slot >> 1);
-  const int which = slot & 1;
-  const int row = pair == 0 ? (which ? N / 2 : 0) : (which ? N - pair : pair);
+  const int row = spec_row_of<N>(tile, slot);
   const int pslot = pair == 0 ? slot : (slot ^ 1);
+  float2* const stage = reinterpret_cast<float2*>(reinterpret_cast<char*>(smem) + TU::B_STAGE_OFF);
+  if constexpr (TU::PREFETCH) {
+    // one thread stages the rows this tile's RK update reads; they land while the
+    // x-FFT of Z runs
+    if (tid == 0) {
+      mbar_arrive_expect_tx(bar, (uint32_t)(NARR * TU::B_ROWS * N * sizeof(float2)));
+      for (int s = 0; s < TU::B_ROWS; ++s) {
+        const size_t ro = (size_t)spec_row_of<N>(tile, s) * N;
+        int k = 0;
+        bulk_g2s(stage + (size_t)(k++ * TU::B_ROWS + s) * N, a.wcur + ro, N * sizeof(float2), bar);
+        if constexpr (MODE >= 1) bulk_g2s(stage + (size_t)(k++ * TU::B_ROWS + s) * N, a.w0 + ro, N * sizeof(float2), bar);
+        if constexpr (PTR) bulk_g2s(stage + (size_t)(k++ * TU::B_ROWS + s) * N, a.fptr + ro, N * sizeof(float2), bar);
+      }
+    }
+  }
+  const float2* const s_wcur = stage + (size_t)slot * N;
+  const float2* const s_w0 = stage + (size_t)(TU::B_ROWS + slot) * N;
+  const float2* const s_fptr = stage + (size_t)((MODE >= 1 ? 2 : 1) * TU::B_ROWS + slot) * N;
   float2* const own0 = smem + (2 * slot) * LDS;
   float2* const own1 = smem + (2 * slot + 1) * LDS;
   const float ky = wn<N>(row);
@@ -234,6 +276,8 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
     }
   }
 
+  if constexpr (TU::PREFETCH) mbar_wait_bounded(bar, parity, a.err, 1);
+
   // RK3 stage update, one cell per iteration (kept rolled: the forcing and
   // integrating-factor code appears once in the kernel, not 16 times)
   {
@@ -246,17 +290,17 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
       const size_t o = rbase + c;
       float2 w;
       if constexpr (MODE < 0) {
-        w = a.wcur[o];
+        w = TU::PREFETCH ? s_wcur[c] : a.wcur[o];
       } else {
         const float kx = wn<N>(c);
         const float k2 = kx * kx + ky * ky;
-        const float2 wc = a.wcur[o];
-        const float2 w0 = MODE == 0 ? wc : a.w0[o];
+        const float2 wc = TU::PREFETCH ? s_wcur[c] : a.wcur[o];
+        const float2 w0 = MODE == 0 ? wc : (TU::PREFETCH ? s_w0[c] : a.w0[o]);
         const bool band = row_band && fabsf(kx) < KCUT;
         const float2 nhat = any_band ? own1[PL::pad(c)] : make_float2(0.f, 0.f);
         float2 rhs = make_float2(-nhat.x, -nhat.y);
         if constexpr (PTR) {
-          if (band) rhs = cadd(rhs, __ldg(a.fptr + o));
+          if (band) rhs = cadd(rhs, TU::PREFETCH ? s_fptr[c] : __ldg(a.fptr + o));
         }
         if (a.stochastic && band && k2 > 0.f) rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
         w = k2 == 0.f ? make_float2(0.f, 0.f) : rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
@@ -295,10 +339,22 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
   }
 }
 
+// initialise the tile barrier of a spectral-row CTA (all threads call; one initialises)
+template <int N> __device__ __forceinline__ uint64_t* spec_barrier_init(float2* smem) {
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + Tune<N>::B_BAR_OFF);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  return bar;
+}
+
 template <int N, int MODE, bool PTR>
 __global__ void __launch_bounds__(Tune<N>::B_THREADS, Tune<N>::B_MINB) k_spec_rows(SpecArgs a) {
-  extern __shared__ float2 smem[];
-  spec_rows_tile<N, MODE, PTR>(a, blockIdx.x, smem);
+  extern __shared__ __align__(16) float2 smem[];
+  uint64_t* bar = spec_barrier_init<N>(smem);
+  spec_rows_tile<N, MODE, PTR>(a, blockIdx.x, smem, bar, 0u);
 }
 
 // ---------------------------------------------------------------------------------------

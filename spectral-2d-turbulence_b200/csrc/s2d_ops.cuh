@@ -28,13 +28,13 @@ template <int N> struct OpsImpl {
     chk(set_smem(k_phys_cols<N, 0>, TU::A_SMEM));
     chk(set_smem(k_phys_cols<N, 1>, TU::A_SMEM));
     chk(set_smem(k_phys_cols<N, 2>, TU::A_SMEM));
-    chk(set_smem(k_spec_rows<N, -1, false>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 0, false>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 1, false>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 2, false>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 0, true>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 1, true>, TU::B_SMEM));
-    chk(set_smem(k_spec_rows<N, 2, true>, TU::B_SMEM));
+    chk(set_smem(k_spec_rows<N, -1, false>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 0, false>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 1, false>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 2, false>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 0, true>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 1, true>, TU::B_SMEM_TOTAL));
+    chk(set_smem(k_spec_rows<N, 2, true>, TU::B_SMEM_TOTAL));
     chk(set_smem(k_fft_rows<N, -1>, TU::ROWS_SMEM));
     chk(set_smem(k_fft_rows<N, +1>, TU::ROWS_SMEM));
     chk(set_smem(k_fft_cols<N, -1>, TU::COLS_SMEM));
@@ -50,18 +50,18 @@ template <int N> struct OpsImpl {
   static void spec_rows(int mode, bool ptr, const SpecArgs& a, cudaStream_t st) {
     const dim3 g(TU::B_GRID), b(TU::B_THREADS);
     switch (mode) {
-      case -1: k_spec_rows<N, -1, false><<<g, b, TU::B_SMEM, st>>>(a); break;
+      case -1: k_spec_rows<N, -1, false><<<g, b, TU::B_SMEM_TOTAL, st>>>(a); break;
       case 0:
-        if (ptr) k_spec_rows<N, 0, true><<<g, b, TU::B_SMEM, st>>>(a);
-        else k_spec_rows<N, 0, false><<<g, b, TU::B_SMEM, st>>>(a);
+        if (ptr) k_spec_rows<N, 0, true><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
+        else k_spec_rows<N, 0, false><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
         break;
       case 1:
-        if (ptr) k_spec_rows<N, 1, true><<<g, b, TU::B_SMEM, st>>>(a);
-        else k_spec_rows<N, 1, false><<<g, b, TU::B_SMEM, st>>>(a);
+        if (ptr) k_spec_rows<N, 1, true><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
+        else k_spec_rows<N, 1, false><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
         break;
       default:
-        if (ptr) k_spec_rows<N, 2, true><<<g, b, TU::B_SMEM, st>>>(a);
-        else k_spec_rows<N, 2, false><<<g, b, TU::B_SMEM, st>>>(a);
+        if (ptr) k_spec_rows<N, 2, true><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
+        else k_spec_rows<N, 2, false><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
         break;
     }
   }
@@ -83,7 +83,7 @@ template <int N> struct OpsImpl {
     o.b_grid = TU::B_GRID;
     o.b_threads = TU::B_THREADS;
     o.a_smem = TU::A_SMEM;
-    o.b_smem = TU::B_SMEM;
+    o.b_smem = TU::B_SMEM_TOTAL;
     o.rows_smem = TU::ROWS_SMEM;
     o.cols_smem = TU::COLS_SMEM;
     o.set_attrs = &set_attrs;
