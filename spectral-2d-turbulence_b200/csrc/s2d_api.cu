@@ -16,6 +16,7 @@
 #include "../../include/s2d.h"
 #include "s2d_aux_kernels.cuh"
 #include "s2d_ops.cuh"
+#include "s2d_tc.cuh"
 
 using namespace s2d;
 
@@ -330,7 +331,10 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   const NOps* ops = ops_for(n);
   if (!ops) return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " outside 32..4096");
   if (dye_scale < 1 || dye_scale > 4) return fail(S2D_ERR_ARG, "dye_scale must be 1..4");
-  if (fft_precision != S2D_FFT_FP32) return fail(S2D_ERR_ARG, "unknown FFT precision");
+  if (fft_precision != S2D_FFT_FP32 && fft_precision != S2D_FFT_TC_F16)
+    return fail(S2D_ERR_ARG, "unknown or unsupported FFT arithmetic (S2D_FFT_FP32, S2D_FFT_TC_F16)");
+  if (fft_precision == S2D_FFT_TC_F16 && n != 1024)
+    return fail(S2D_ERR_UNSUPPORTED_N, "the tensor-core FFT is built for N = 1024");
   if (int rc = check_device(device)) return rc;
   DeviceGuard guard(device);
   s2d_solver* s = new s2d_solver();
@@ -384,6 +388,12 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(ops->set_attrs(), "kernel attributes");
   TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
+  if (fft_precision == S2D_FFT_TC_F16) {
+    TRY(cudaFuncSetAttribute(tc::k_fft_tc<0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
+    TRY(cudaFuncSetAttribute(tc::k_fft_tc<0, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
+    TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
+    TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
+  }
   // zero everything the reference's fresh buffers hold as zero
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
   TRY(cudaMemsetAsync(s->packA, 0, cbytes, s->stream), "memset");
@@ -531,6 +541,21 @@ extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
 static inline unsigned cells_grid(int n) { return (unsigned)(((size_t)n * n + 255) / 256); }
 
 static int enqueue_fft2(s2d_solver* s, float2* buf, int sign) {
+  if (s->fft_precision == S2D_FFT_TC_F16) {
+    // tensor-core DFT-GEMM passes, 8 lines of 1024 per CTA
+    const dim3 g(1024 / tc::kTcLines), b(tc::kTcThreads);
+    if (sign < 0) {
+      tc::k_fft_tc<0, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      S2D_LAUNCHED();
+      tc::k_fft_tc<1, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+    } else {
+      tc::k_fft_tc<0, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      S2D_LAUNCHED();
+      tc::k_fft_tc<1, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+    }
+    S2D_LAUNCHED();
+    return S2D_OK;
+  }
   s->ops->fft_rows(sign, buf, s->tw, s->stream);
   S2D_LAUNCHED();
   s->ops->fft_cols(sign, buf, s->tw, s->stream);

@@ -47,9 +47,11 @@ template <int N_> struct Tune {
   static constexpr int B_MINB = 65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1;
   static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
   static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
-  // rows the spectral-row kernel stages by TMA bulk copy (wcur, w0, pointer force),
-  // after the exchange lines; off at N = 4096, where they would not fit
-  static constexpr bool PREFETCH = N <= 2048;
+  // rows the spectral-row kernel can stage by TMA bulk copy (wcur, w0, pointer force)
+  // after the exchange lines.  Off: measured at 1024^2 the 48 KB of staging halves the
+  // resident CTAs (4 -> 2 per SM) and the kernel slows from 30 to 40 us, more than the
+  // overlap with the x-FFT of Z recovers.
+  static constexpr bool PREFETCH = false;
   static constexpr size_t B_STAGE_OFF = B_SMEM;
   static constexpr size_t B_STAGE_BYTES = PREFETCH ? sizeof(float2) * 3 * B_ROWS * N : 0;
   static constexpr size_t B_BAR_OFF = B_STAGE_OFF + B_STAGE_BYTES;

@@ -379,3 +379,32 @@ def test_profiler_counts_every_kernel_class(pkg, graph):
         assert all(p[k][0] > 0 for k in ("phys_cols", "spec_rows", "dye"))
     finally:
         s.destroy()
+
+
+# ---------------------------------------------------------------- tensor-core DFT-GEMM FFT
+def test_tc_fft2_matches_numpy(pkg):
+    """Split-FP16 tcgen05 DFT-GEMM 2D FFT at 1024^2 vs FP64 numpy (target rel L2 <= 1e-5)."""
+    n = 1024
+    rng = np.random.default_rng(7)
+    a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    s = pkg.Solver.create(n=n, dyeScale=1, fft="tc-f16")
+    try:
+        s.setBuffer("packB", a)
+        s.fft.forward(None, "packB")
+        fwd = s.getBuffer("packB")
+        err_f = rel_l2(fwd, np.fft.fft2(a.astype(np.complex128)))
+        s.fft.inverse(None, "packB")
+        err_rt = rel_l2(s.getBuffer("packB"), a)
+        s.setBuffer("packB", a)
+        s.fft.inverse(None, "packB")
+        err_i = rel_l2(s.getBuffer("packB"), np.fft.ifft2(a.astype(np.complex128)))
+        print(f"tc fft2 rel L2: forward {err_f:.3e} inverse {err_i:.3e} round trip {err_rt:.3e}")
+        assert err_f <= 1e-5 and err_i <= 1e-5 and err_rt <= 2e-5
+    finally:
+        s.destroy()
+
+
+def test_tc_precision_only_at_1024(pkg):
+    with pytest.raises(pkg.S2DError) as ei:
+        pkg.Solver.create(n=512, fft="tc-f16")
+    assert ei.value.status == -2
