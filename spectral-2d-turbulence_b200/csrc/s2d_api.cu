@@ -393,6 +393,12 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
     TRY(cudaFuncSetAttribute(tc::k_fft_tc<0, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
     TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
     TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
+    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
+        "tc");
+    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
+        "tc");
+    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
+        "tc");
   }
   // zero everything the reference's fresh buffers hold as zero
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
@@ -596,6 +602,19 @@ static PhysArgs phys_args(s2d_solver* s, int reduce) {
   return a;
 }
 
+// the physical-column stage: tensor-core y-transforms when the solver was created
+// with S2D_FFT_TC_F16 (1024^2 only), else the FP32 whole-line kernel
+static void enqueue_phys_cols(s2d_solver* s, int mode, const PhysArgs& a) {
+  if (s->fft_precision == S2D_FFT_TC_F16) {
+    const dim3 g(tc::kTcColsGrid), b(tc::kTcThreads);
+    if (mode == 0) tc::k_phys_cols_tc<0><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
+    else if (mode == 1) tc::k_phys_cols_tc<1><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
+    else tc::k_phys_cols_tc<2><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
+  } else {
+    s->ops->phys_cols(mode, a, s->stream);
+  }
+}
+
 extern "C" int s2d_encode_reduce(s2d_solver* s);
 
 extern "C" int s2d_encode_prime(s2d_solver* s) {
@@ -603,7 +622,7 @@ extern "C" int s2d_encode_prime(s2d_solver* s) {
   DeviceGuard guard(s->dev);
   if (int rc = enqueue_pack_prime(s)) return rc;
   PhysArgs a = phys_args(s, 1);
-  s->ops->phys_cols(0, a, s->stream);
+  enqueue_phys_cols(s, 0, a);
   S2D_LAUNCHED();
   s->reduced_valid = true;
   if (int rc = s2d_encode_reduce(s)) return rc;
@@ -628,7 +647,7 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     {
       ProfScope ps(s, S2D_PROF_PHYS_COLS);
       PhysArgs pa = phys_args(s, st == 2 ? 1 : 0);
-      s->ops->phys_cols(st == 2 ? 2 : 1, pa, s->stream);
+      enqueue_phys_cols(s, st == 2 ? 2 : 1, pa);
       S2D_LAUNCHED();
     }
     ProfScope ps(s, S2D_PROF_SPEC_ROWS);

@@ -156,49 +156,55 @@ __device__ __forceinline__ float phys_cols_tile(const PhysArgs& a, int tile, flo
   return speed;
 }
 
+// CTA max of |u|+|v| into partials[blockIdx.x]; with a.reduce the last CTA to finish
+// reduces the partials and writes [dt, speed] into a.dt_out (last-CTA-done ticket).
+// Every thread of a CTA of NTHREADS calls it.
+template <int NTHREADS>
+__device__ __forceinline__ void cols_speed_finalize(const PhysArgs& a, float speed) {
+  __shared__ float red[32];
+  __shared__ int last;
+  const int tid = threadIdx.x;
+  speed = warp_max(speed);
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0) red[warp] = speed;
+  __syncthreads();
+  if (warp == 0) {
+    float s = lane < (NTHREADS + 31) / 32 ? red[lane] : 0.f;
+    s = warp_max(s);
+    if (lane == 0) {
+      a.partials[blockIdx.x] = s;
+      int is_last = 0;
+      if (a.reduce) {
+        __threadfence();
+        const unsigned k = atomicAdd(a.ticket, 1u);
+        is_last = (k == gridDim.x - 1);
+      }
+      last = is_last;
+    }
+  }
+  __syncthreads();
+  if (last) {
+    float s = 0.f;
+    for (int i = tid; i < (int)gridDim.x; i += blockDim.x) s = fmaxf(s, __ldcg(a.partials + i));
+    s = warp_max(s);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+      float m = 0.f;
+      for (int i = 0; i < (NTHREADS + 31) / 32; ++i) m = fmaxf(m, red[i]);
+      a.dt_out[0] = cfl_dt(*a.params, m);
+      a.dt_out[1] = m;
+      *a.ticket = 0u;
+    }
+  }
+}
+
 template <int N, int MODE>
 __global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_cols(PhysArgs a) {
   using TU = Tune<N>;
   extern __shared__ float2 smem[];
-  float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
-  const int tid = threadIdx.x;
-  if constexpr (MODE != 1) {
-    __shared__ float red[32];
-    __shared__ int last;
-    speed = warp_max(speed);
-    const int lane = tid & 31, warp = tid >> 5;
-    if (lane == 0) red[warp] = speed;
-    __syncthreads();
-    if (warp == 0) {
-      float s = lane < (TU::A_THREADS + 31) / 32 ? red[lane] : 0.f;
-      s = warp_max(s);
-      if (lane == 0) {
-        a.partials[blockIdx.x] = s;
-        int is_last = 0;
-        if (a.reduce) {
-          __threadfence();
-          const unsigned k = atomicAdd(a.ticket, 1u);
-          is_last = (k == gridDim.x - 1);
-        }
-        last = is_last;
-      }
-    }
-    __syncthreads();
-    if (last) {
-      float s = 0.f;
-      for (int i = tid; i < (int)gridDim.x; i += blockDim.x) s = fmaxf(s, __ldcg(a.partials + i));
-      s = warp_max(s);
-      if (lane == 0) red[warp] = s;
-      __syncthreads();
-      if (tid == 0) {
-        float m = 0.f;
-        for (int i = 0; i < (TU::A_THREADS + 31) / 32; ++i) m = fmaxf(m, red[i]);
-        a.dt_out[0] = cfl_dt(*a.params, m);
-        a.dt_out[1] = m;
-        *a.ticket = 0u;
-      }
-    }
-  }
+  const float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
+  if constexpr (MODE != 1) cols_speed_finalize<TU::A_THREADS>(a, speed);
 }
 
 // ---------------------------------------------------------------------------------------

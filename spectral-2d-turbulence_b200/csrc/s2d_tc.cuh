@@ -20,6 +20,7 @@
 #include <cuda_fp16.h>
 #include "s2d_async.cuh"
 #include "s2d_device.cuh"
+#include "s2d_kernels.cuh"
 
 namespace s2d {
 namespace tc {
@@ -190,11 +191,15 @@ static_assert(1024 * kTcStageLd * 8 <= kTcMisc, "output staging must fit over th
 // On return, warp w (line w) thread `lane` (k2) holds X[k2 + 32 k1] in x[k1]
 // (unscaled).  `tmem` holds 128 columns; `phase` is the barrier's next parity
 // (two phases are consumed).
-template <int SIGN>
+// NBLK = 2: 8 lines (all warps hold a line); NBLK = 1: 4 lines (warps 0-3), the
+// other warps only join the barriers.  bhi/blo: byte offsets of the DFT32 planes.
+template <int SIGN, int NBLK = 2>
 __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t* bar, uint32_t phase, float scale,
-                                              const float2* __restrict__ tw, int* err, float2 (&x)[32]) {
+                                              const float2* __restrict__ tw, int* err, float2 (&x)[32],
+                                              int bhi = kTcBHi, int blo = kTcBLo) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int blk = warp >> 2, quad = warp & 3;
+  const bool active = blk < NBLK;
   unsigned* maxw = reinterpret_cast<unsigned*>(sm + kTcMisc + 12);
   const uint32_t base = smem_u32(sm);
   // ---- step A: DFT32 over n2 for every row (line, n1)
@@ -203,9 +208,9 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
   __syncthreads();
   if (tid == 0) {
     fence_after_sync();
-    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + kTcBHi, base + kTcBLo);
-    issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + kTcBHi,
-                   base + kTcBLo);
+    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
+    if (NBLK == 2)
+      issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase, err, 2);
@@ -213,14 +218,19 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
   // row (line = warp, n1 = lane): Y[n1][k2] for k2 = 0..31 in columns 64*blk + 2k2 (+1)
   float y[64];
   const uint32_t lane_base = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(64 * blk);
+  if (active) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    float v[16];
-    tmem_ld16(lane_base + 16 * c, v);
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(lane_base + 16 * c, v);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) y[16 * c + i] = v[i];
+      for (int i = 0; i < 16; ++i) y[16 * c + i] = v[i];
+    }
+    tmem_wait_ld();
+  } else {
+#pragma unroll
+    for (int i = 0; i < 64; ++i) y[i] = 0.f;
   }
-  tmem_wait_ld();
   // twiddle W_1024^{SIGN n1 k2}
   float mx = 0.f;
 #pragma unroll
@@ -239,30 +249,35 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
   // ---- step C operand: rows (line, k2), K = n1 (this thread's lane)
   char* a_hi = sm + kTcAHi;
   char* a_lo = sm + kTcALo;
+  if (active) {
 #pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2) put_c(a_hi, a_lo, warp * 32 + k2, lane, y[2 * k2] * scale2, y[2 * k2 + 1] * scale2);
+    for (int k2 = 0; k2 < 32; ++k2)
+      put_c(a_hi, a_lo, warp * 32 + k2, lane, y[2 * k2] * scale2, y[2 * k2 + 1] * scale2);
+  }
   fence_proxy_async();
   fence_before_sync();
   __syncthreads();
   if (tid == 0) {
     fence_after_sync();
-    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + kTcBHi, base + kTcBLo);
-    issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + kTcBHi,
-                   base + kTcBLo);
+    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
+    if (NBLK == 2)
+      issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase ^ 1u, err, 3);
   fence_after_sync();
   // row (line = warp, k2 = lane): X[k2 + 32 k1] in columns 64*blk + 2k1 (+1)
   const float inv = 1.f / (scale * scale2);   // exact: both are powers of two
+  if (active) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    float v[16];
-    tmem_ld16(lane_base + 16 * c, v);
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(lane_base + 16 * c, v);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x[8 * c + i] = make_float2(v[2 * i] * inv, v[2 * i + 1] * inv);
+      for (int i = 0; i < 8; ++i) x[8 * c + i] = make_float2(v[2 * i] * inv, v[2 * i + 1] * inv);
+    }
+    tmem_wait_ld();
   }
-  tmem_wait_ld();
 }
 
 // Standalone 2D-FFT pass over 8 lines of a 1024 x 1024 field: AXIS 0 = rows
@@ -330,6 +345,134 @@ __global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const float
     fence_after_sync();
     tmem_dealloc(tmem, 128);
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// Fused physical-column stage at 1024^2 with both y-transforms on the tensor cores
+// (the tcgen05 counterpart of k_phys_cols): a CTA owns 4 columns x0..x0+3.
+//   lines 0-3 = PA columns, 4-7 = PB columns -> one 8-line inverse transform
+//   warps 4-7 hand v(y) to warps 0-3 through shared memory
+//   warps 0-3 form (u omega, v omega) -> one 4-line forward transform -> in-band Z rows
+// MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage (+ velocity, speed).
+// Shared memory after the inverse transform (the operands are dead once its second
+// GEMM has completed): v exchange over the block-1 hi plane, (u, v) staging over the
+// block-1 lo plane and the inverse DFT32 planes, forward operands in block 0, Z
+// staging over block 0.
+constexpr int kTcCols = 4;
+constexpr int kTcColsGrid = 1024 / kTcCols;
+constexpr int kTcColsBHi = kTcSmem;                      // forward DFT32 planes, after the misc words
+constexpr int kTcColsBLo = kTcSmem + kBBytes;
+constexpr int kTcColsSmem = kTcSmem + 2 * kBBytes;
+constexpr int kTcColsExch = kBlockBytes;                 // float [4][1024]
+constexpr int kTcColsVel = 3 * kBlockBytes;              // float2 [1024][4], up to kTcMisc
+static_assert(kTcColsVel + 1024 * kTcCols * 8 <= kTcMisc, "velocity staging overlaps the misc words");
+static_assert(kTcColsBHi % 16 == 0, "descriptor base must be 16-byte aligned");
+
+// (y, col) -> float2 slot of a [1024][4] staging tile; the XOR spreads a warp's
+// fixed-column, consecutive-y writes over all banks
+__device__ __forceinline__ int cols_stage_idx(int y, int col) { return 4 * y + (col ^ ((y >> 2) & 3)); }
+
+template <int MODE>
+__global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, int* err) {
+  constexpr int N = 1024;
+  extern __shared__ __align__(1024) char sm[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTcMisc);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 8);
+  unsigned* maxw = reinterpret_cast<unsigned*>(sm + kTcMisc + 12);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int x0 = blockIdx.x * kTcCols;
+  if (warp == 0) {
+    tmem_alloc(tslot, 128);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  build_dft32<+1>(sm + kTcBHi, sm + kTcBLo, a.tw);
+  if (MODE != 0) build_dft32<-1>(sm + kTcColsBHi, sm + kTcColsBLo, a.tw);
+  // load: thread (line g, n1 t) takes the pack at ky = t + 32 n2 -- one operand row
+  const int g = tid & 7, t = tid >> 3;
+  const float2* src = (g < kTcCols ? a.pa : a.pb) + x0 + (g & (kTcCols - 1));
+  float2 v[32];
+  float mx = 0.f;
+#pragma unroll
+  for (int n2 = 0; n2 < 32; ++n2) {
+    v[n2] = __ldcs(src + (size_t)(t + 32 * n2) * N);
+    mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
+  }
+  const float scale = pow2_scale(cta_max(mx, maxw));
+#pragma unroll
+  for (int n2 = 0; n2 < 32; ++n2) put_c(sm + kTcAHi, sm + kTcALo, g * 32 + t, n2, v[n2].x * scale, v[n2].y * scale);
+  __syncthreads();   // the TMEM address written by warp 0 is visible to all
+  const uint32_t tmem = *tslot;
+  float2 x[32];
+  fft1024_gemms<+1, 2>(sm, tmem, bar, 0u, scale, a.tw, err, x);
+  // warp w < 4: (omega, u) of column x0 + w at y = lane + 32 k1; warp 4 + w: (v, 0)
+  float* sv = reinterpret_cast<float*>(sm + kTcColsExch);
+  if (warp >= kTcCols) {
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) sv[(warp - kTcCols) * N + lane + 32 * k1] = x[k1].x;
+  }
+  __syncthreads();
+  float speed = 0.f, mz = 0.f;
+  float2* svel = reinterpret_cast<float2*>(sm + kTcColsVel);
+  if (warp < kTcCols) {
+#pragma unroll
+    for (int k1 = 0; k1 < 32; ++k1) {
+      const int y = lane + 32 * k1;
+      const float om = x[k1].x, u = x[k1].y, w = sv[warp * N + y];
+      if (MODE != 1) {
+        svel[cols_stage_idx(y, warp)] = make_float2(u, w);
+        speed = fmaxf(speed, fabsf(u) + fabsf(w));
+      }
+      x[k1] = make_float2(u * om, w * om);
+      mz = fmaxf(mz, fmaxf(fabsf(x[k1].x), fabsf(x[k1].y)));
+    }
+  }
+  if (MODE != 0) {
+    const float scale_z = pow2_scale(cta_max(mz, maxw));   // its barriers also publish svel
+    if (MODE == 2) {
+#pragma unroll 4
+      for (int i = tid; i < N * kTcCols; i += kTcThreads) {
+        const int y = i >> 2, c = i & 3;
+        a.vel[(size_t)y * N + x0 + c] = svel[cols_stage_idx(y, c)];
+      }
+    }
+    // forward operand: rows (line = warp, n1 = lane), K = n2 = k1 (block 0 only)
+    if (warp < kTcCols) {
+#pragma unroll
+      for (int k1 = 0; k1 < 32; ++k1)
+        put_c(sm + kTcAHi, sm + kTcALo, warp * 32 + lane, k1, x[k1].x * scale_z, x[k1].y * scale_z);
+    }
+    fft1024_gemms<-1, 1>(sm, tmem, bar, 0u, scale_z, a.tw, err, x, kTcColsBHi, kTcColsBLo);
+    // warp w < 4: Z(ky = lane + 32 k1, x0 + w); stage for row-contiguous stores of the in-band rows
+    float2* sz = reinterpret_cast<float2*>(sm);
+    if (warp < kTcCols) {
+#pragma unroll
+      for (int k1 = 0; k1 < 32; ++k1) sz[cols_stage_idx(lane + 32 * k1, warp)] = x[k1];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
+      const int row = i >> 2, c = i & 3;
+      if (fabsf(wn<N>(row)) < Tune<N>::KCUT) a.z[(size_t)row * N + x0 + c] = sz[cols_stage_idx(row, c)];
+    }
+  } else {
+    __syncthreads();
+#pragma unroll 4
+    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
+      const int y = i >> 2, c = i & 3;
+      a.vel[(size_t)y * N + x0 + c] = svel[cols_stage_idx(y, c)];
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    tmem_dealloc(tmem, 128);
+  }
+  if (MODE != 1) cols_speed_finalize<kTcThreads>(a, speed);
 }
 
 }  // namespace tc

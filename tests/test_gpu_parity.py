@@ -408,3 +408,109 @@ def test_tc_precision_only_at_1024(pkg):
     with pytest.raises(pkg.S2DError) as ei:
         pkg.Solver.create(n=512, fft="tc-f16")
     assert ei.value.status == -2
+
+
+def _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt):
+    s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+    s.configure(config(beta=beta, drag=mu, viscosity=rate_for(nu_h, n, p), hyperP=p))
+    load_state(s, w_in)
+    set_fixed_dt(s, dt)
+    s.setSplats([])
+    return s
+
+
+@pytest.mark.parametrize("beta", [0.0, 10.0])
+def test_tc_fused_step_vs_oracle(pkg, beta):
+    """Fused RK3 step with the tensor-core column stage (split FP16 DFT-GEMMs) vs the
+    FP64 oracle at 1024^2: rel L2 <= 1e-5 after one step, <= 3e-5 after five."""
+    n, mu, p, dt, amp = 1024, 1e-2, 4, 1e-3, 8.0
+    nu_h = 1.0 / (n / 3.0) ** 8
+    ref = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
+    ref.set_vorticity(random_field(n, k0=n / 8, seed=11, amplitude=amp))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = _tc_case_solver(pkg, "tc-f16", n, beta, mu, nu_h, p, w_in, dt)
+    try:
+        s.encodeStep()
+        ref.step(dt=dt)
+        err1 = rel_l2(current_state(s), ref.w)
+        for _ in range(4):
+            s.encodeStep()
+            ref.step(dt=dt)
+        err5 = rel_l2(current_state(s), ref.w)
+        print(f"tc fused step rel L2: 1 step {err1:.3e}, 5 steps {err5:.3e}")
+        assert err1 <= 1e-5, f"one step rel L2 {err1:.3e}"
+        assert err5 <= 3e-5, f"five steps rel L2 {err5:.3e}"
+    finally:
+        s.destroy()
+
+
+def test_tc_prime_velocity_and_dt(pkg):
+    """encodePrime through the tensor-core column stage: velocity vs the FP32 path and
+    the CFL dt from its max |u|+|v|."""
+    n = 1024
+    w = random_field(n, k0=40, seed=5, amplitude=6.0)
+    out = {}
+    for fft in ("fp32", "tc-f16"):
+        s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+        try:
+            s.configure(config(viscosity=1.0, cfl=0.5, dtMax=1.0))
+            s.seedPhysical(w)
+            s.encodePrime()
+            out[fft] = (s.getBuffer("vel"), s.getBuffer("dt"))
+        finally:
+            s.destroy()
+    v32, d32 = out["fp32"]
+    vtc, dtc = out["tc-f16"]
+    assert rel_l2(vtc, v32) <= 1e-5
+    assert abs(float(dtc[1]) / float(d32[1]) - 1) <= 1e-5
+    assert abs(float(dtc[0]) / float(d32[0]) - 1) <= 1e-5
+
+
+def test_tc_forced_run_tracks_fp32(pkg):
+    """Forced, adaptive-dt run with dye (the 1024^2 benchmark configuration) through the
+    tensor-core column stage stays within 1e-5 (rel L2) of the FP32 path after 5 steps,
+    and the dt chain agrees."""
+    n = 1024
+    w = random_field(n, k0=14, seed=1, amplitude=6.0)
+    out = {}
+    for fft in ("fp32", "tc-f16"):
+        s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+        try:
+            s.configure(config(viscosity=1.0, hyperP=4, drag=1e-2, forceAmp=0.1, forceK=64.0, forceWidth=2.0,
+                               cfl=0.5, dtMax=1e-3))
+            s.reset({"field": w, "dyePattern": "bands"})
+            s.step(5, dye=True, reduce=True, graph=True)
+            out[fft] = (current_state(s), s.getBuffer("dt"), s.getBuffer("vel"))
+        finally:
+            s.destroy()
+    e_state = rel_l2(out["tc-f16"][0], out["fp32"][0])
+    e_vel = rel_l2(out["tc-f16"][2], out["fp32"][2])
+    print(f"tc vs fp32 after 5 forced steps: state {e_state:.3e} vel {e_vel:.3e}")
+    assert e_state <= 1e-5 and e_vel <= 1e-5
+    assert abs(float(out["tc-f16"][1][0]) / float(out["fp32"][1][0]) - 1) <= 1e-5
+
+
+def test_tc_taylor_green_decay_rate(pkg):
+    """Taylor-Green through the tensor-core step at 1024^2: the (2,2) mode decays as
+    exp(-nu |k|^2 t) to 1e-5 (the Jacobian error of the split-FP16 transforms feeds
+    straight into that mode)."""
+    n, nu, dt, steps = 1024, 1e-3, 2e-3, 200
+    xs = np.arange(n) * 2 * np.pi / n
+    gx, gy = np.meshgrid(xs, xs, indexing="xy")
+    s = pkg.Solver.create(n=n, dyeScale=1, fft="tc-f16")
+    try:
+        s.configure(config(viscosity=rate_for(nu, n, 1), hyperP=1))
+        s.seedPhysical(6.0 * np.cos(2 * gx) * np.cos(2 * gy))
+        w0 = current_state(s)[2, 2]
+        set_fixed_dt(s, dt)
+        for _ in range(steps):
+            s.encodeStep()
+        w1 = current_state(s)[2, 2]
+        nu_h = s.paramsF[2]
+        expected = np.exp(-float(nu_h) * 8.0 * dt * steps)
+        err = abs(abs(w1 / w0) / expected - 1)
+        print(f"tc Taylor-Green decay-rate error {err:.3e}")
+        assert err <= 1e-5
+    finally:
+        s.destroy()
