@@ -347,6 +347,11 @@ def run_ours(args):
     finite = d is not None and all(map(lambda v: v == v, [d["energy"], d["enstrophy"], d["dt"]]))
     solver.destroy()
 
+    # ---- the same step with the tensor-core (split FP16 DFT-GEMM) column stage
+    tc = None
+    if not args.no_tc:
+        tc = run_tc_leg(pkg, torch, world, rank, dev, args, value, world * args.steps / (ms_rk3 / 1e3))
+
     # ---- batched ensemble: 256 instances of 256^2 (sharded across ranks)
     ens = None
     if not args.no_ensemble:
@@ -374,6 +379,7 @@ def run_ours(args):
             "gpu_launches": args.steps * 10,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "tc_vs_fp32": tc,
             "ensemble": ens,
         }
         print(json.dumps(line), flush=True)
@@ -381,6 +387,76 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def _timed_steps(solver, stream, torch, steps, dye):
+    solver.step(3, dye=dye, reduce=True, graph=True, relatch=True)
+    solver.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    solver.step(steps, dye=dye, reduce=True, graph=True, relatch=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1)
+
+
+def _bench_solver(pkg, dev, fft, seed):
+    s = pkg.Solver.create(device=dev, n=N, dyeScale=DYE_SCALE, fft=fft)
+    s.configure(CFG)
+    s.reset({"k0": 14, "amplitude": 0, "seed": 1, "dyePattern": "bands"})
+    s.seedBand(4.0, 12.0, rms=1.0, seed=seed)
+    return s
+
+
+def tc_divergence(pkg, dev, steps=10):
+    """rel L2 between the FP32 and the tensor-core step after 1 and `steps` steps of the
+    benchmark configuration from the same seeded state (adaptive dt, forcing on)."""
+    import numpy as np
+    out = {}
+    for fft in ("fp32", "tc-f16"):
+        s = _bench_solver(pkg, dev, fft, 1)
+        try:
+            s.step(1, dye=False, reduce=True, graph=False)
+            one = s.getBuffer(f"state{s.phase}")
+            s.step(steps - 1, dye=False, reduce=True, graph=False)
+            many = s.getBuffer(f"state{s.phase}")
+            out[fft] = (one.astype(np.complex128), many.astype(np.complex128))
+        finally:
+            s.destroy()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return {"1_step": rel(out["tc-f16"][0], out["fp32"][0]),
+            f"{steps}_steps": rel(out["tc-f16"][1], out["fp32"][1])}
+
+
+def run_tc_leg(pkg, torch, world, rank, dev, args, fp32_value, fp32_rk3):
+    """Time the benchmark step with fft='tc-f16' (both y-transforms of every RK stage as
+    split-FP16 tcgen05 DFT-GEMMs) exactly like the FP32 step, and measure how far it
+    drifts from the FP32 step."""
+    solver = _bench_solver(pkg, dev, "tc-f16", 1 + rank)
+    stream = torch.cuda.ExternalStream(solver.stream, device=dev)
+    solver.step(max(args.warmup, 6), dye=True, reduce=True, graph=True, relatch=True)
+    solver.synchronize()
+    barrier(world)
+    ms = max_over_ranks(_timed_steps(solver, stream, torch, args.steps, True), world)
+    ms_rk3 = max_over_ranks(_timed_steps(solver, stream, torch, args.steps, False), world)
+    ksteps = min(args.steps, 60)
+    solver.profile(True)
+    solver.step(6, dye=False, reduce=True, graph=True, relatch=True)
+    solver.profileRead()
+    solver.step(ksteps, dye=False, reduce=True, graph=True, relatch=True)
+    prof = solver.profileRead()
+    solver.profile(False)
+    solver.destroy()
+    value = world * args.steps / (ms / 1e3)
+    rk3 = world * args.steps / (ms_rk3 / 1e3)
+    return {"fft": "split FP16 hi+lo tcgen05 DFT-GEMM (y-transforms); FP32 row transforms",
+            "steps_per_s": value, "rk3_only_steps_per_s": rk3,
+            "fp32_steps_per_s": fp32_value, "fp32_rk3_only_steps_per_s": fp32_rk3,
+            "rk3_speedup_vs_fp32": rk3 / fp32_rk3, "speedup_vs_fp32": value / fp32_value,
+            "per_kernel_ms_per_step": {k: prof[k][0] / ksteps for k in prof},
+            "rel_l2_vs_fp32": tc_divergence(pkg, dev)}
 
 
 def working_set(n, m):
@@ -432,6 +508,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tc", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
