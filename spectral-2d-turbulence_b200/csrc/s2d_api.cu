@@ -144,6 +144,7 @@ struct s2d_solver {
   double* seed_parts = nullptr;
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
   int* err = nullptr;                 // device error word (bounded waits that gave up)
+  char* tctab = nullptr;              // tensor-core DFT32 planes + twiddle matrix (fft 'tc-f16')
   ushort4* dye[3] = {nullptr, nullptr, nullptr};
   // pinned readback staging (copyDiagnostics)
   double* h_diag = nullptr;
@@ -212,7 +213,7 @@ static void free_solver(s2d_solver* s) {
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
                       s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->dye[0], s->dye[1], s->dye[2]};
+                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
   void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
@@ -414,6 +415,11 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream), "memset");
   k_twiddles<<<(n + 255) / 256, 256, 0, s->stream>>>(s->tw, n);
   TRY(cudaGetLastError(), "twiddle kernel");
+  if (fft_precision == S2D_FFT_TC_F16) {
+    TRY(cudaMalloc(&s->tctab, tc::kTabBytes), "tensor-core tables");
+    tc::k_tc_tables<<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
+    TRY(cudaGetLastError(), "tensor-core table kernel");
+  }
   // an unconfigured solver has all-zero parameters apart from the grid constants
   s->hp = DevParams{};
   s->hp.n = n;
@@ -551,13 +557,13 @@ static int enqueue_fft2(s2d_solver* s, float2* buf, int sign) {
     // tensor-core DFT-GEMM passes, 8 lines of 1024 per CTA
     const dim3 g(1024 / tc::kTcLines), b(tc::kTcThreads);
     if (sign < 0) {
-      tc::k_fft_tc<0, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      tc::k_fft_tc<0, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
       S2D_LAUNCHED();
-      tc::k_fft_tc<1, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      tc::k_fft_tc<1, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
     } else {
-      tc::k_fft_tc<0, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      tc::k_fft_tc<0, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
       S2D_LAUNCHED();
-      tc::k_fft_tc<1, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tw, s->err);
+      tc::k_fft_tc<1, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
     }
     S2D_LAUNCHED();
     return S2D_OK;
@@ -607,9 +613,9 @@ static PhysArgs phys_args(s2d_solver* s, int reduce) {
 static void enqueue_phys_cols(s2d_solver* s, int mode, const PhysArgs& a) {
   if (s->fft_precision == S2D_FFT_TC_F16) {
     const dim3 g(tc::kTcColsGrid), b(tc::kTcThreads);
-    if (mode == 0) tc::k_phys_cols_tc<0><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
-    else if (mode == 1) tc::k_phys_cols_tc<1><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
-    else tc::k_phys_cols_tc<2><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->err);
+    if (mode == 0) tc::k_phys_cols_tc<0><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
+    else if (mode == 1) tc::k_phys_cols_tc<1><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
+    else tc::k_phys_cols_tc<2><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
   } else {
     s->ops->phys_cols(mode, a, s->stream);
   }

@@ -4,12 +4,16 @@
 //   x[n1 + 32 n2] --(DFT32 over n2, a GEMM)--> Y[n1][k2]
 //   Y *= W_1024^{n1 k2}                        (FP32 twiddle, CUDA cores)
 //   Y --(DFT32 over n1, a GEMM)--> X[k2 + 32 k1]
-// Each DFT32 is a real GEMM D[M x 64] = A[M x 64] . B[64 x 64]: rows of A are
-// (line, fixed index) with the 32 complex inputs as 64 interleaved (re, im)
-// values along K; B is the real block form of the 32 x 32 DFT matrix.
+// Each DFT32 is a real GEMM D[M x 64] = A[M x 64] . B[64 x 64]: row r of A is
+// (fixed index i, line l) with r = i * L + l for L lines, holding the 32 complex
+// inputs as 64 interleaved (re, im) values along K; B is the real block form of
+// the 32 x 32 DFT matrix.  The interleaved row order makes every operand store of
+// a warp land in distinct shared-memory banks.
 // Operands are FP16 split as hi + lo with x ~= hi + lo and the three products
-// hi.hi + hi.lo + lo.hi accumulated in FP32 in tensor memory (TMEM); a per-CTA
-// power-of-two scale keeps every operand inside FP16 range (scaling is exact).
+// hi.hi + hi.lo + lo.hi accumulated in FP32 in tensor memory (TMEM).  A per-CTA
+// power-of-two scale keeps the first GEMM's operand inside FP16 range; the
+// second GEMM's operand is bounded by 32 x the first (|Y| <= sum |x|), so it
+// takes that scale times 2^-5 without another reduction (scaling is exact).
 //
 // tcgen05 usage: one elected thread issues tcgen05.mma (cta_group::1,
 // kind::f16, M = 128, N = 64, K = 16, A and B K-major in shared memory, no
@@ -161,7 +165,7 @@ __device__ __forceinline__ float cta_max(float v, unsigned* word) {
   return __uint_as_float(*word);
 }
 
-// power-of-two scale that maps max |x| to at most 2^14 (FP16 max is 65504)
+// power-of-two scale that maps max |x| into [2^13, 2^14) (FP16 max is 65504)
 __device__ __forceinline__ float pow2_scale(float maxabs) {
   if (!(maxabs > 0.f) || !isfinite(maxabs)) return 1.f;
   const int e = ilogbf(maxabs);                       // maxabs in [2^e, 2^(e+1))
@@ -174,135 +178,224 @@ __device__ __forceinline__ float pow2_scale(float maxabs) {
 namespace s2d {
 namespace tc {
 
-// shared-memory plan of the 8-line transform CTA
-constexpr int kTcLines = 8;                       // lines per CTA: two M = 128 blocks
-constexpr int kTcThreads = 256;
-constexpr int kTcAHi = 0;                         // 2 blocks, hi plane
-constexpr int kTcALo = 2 * kBlockBytes;           // 2 blocks, lo plane
-constexpr int kTcBHi = 4 * kBlockBytes;
+// ------------------------------------------------------------------ shared-memory plan
+constexpr int kTcThreads = 256;                   // 8 warps
+constexpr int kTcAHi = 0;                         // up to 2 M-blocks, hi plane
+constexpr int kTcALo = 2 * kBlockBytes;           // up to 2 M-blocks, lo plane
+constexpr int kTcBHi = 4 * kBlockBytes;           // inverse (+1) DFT32, hi / lo planes
 constexpr int kTcBLo = 4 * kBlockBytes + kBBytes;
-constexpr int kTcMisc = 4 * kBlockBytes + 2 * kBBytes;   // mbarrier, TMEM slot, max word
-constexpr int kTcSmem = kTcMisc + 64;
-constexpr int kTcStageLd = 9;                     // padded row (8 lines + 1) of the output staging
-static_assert(1024 * kTcStageLd * 8 <= kTcMisc, "output staging must fit over the operands");
+constexpr int kTcMisc = 4 * kBlockBytes + 2 * kBBytes;   // mbarriers, TMEM slot, per-warp max slots
+constexpr int kTcFwdBHi = kTcMisc + 128;          // forward (-1) DFT32, hi / lo planes
+constexpr int kTcFwdBLo = kTcFwdBHi + kBBytes;
+constexpr int kTcTw = kTcFwdBLo + kBBytes;        // W_1024^{n1 k2}, rows n1 padded to 34 entries
+constexpr int kTcTwLd = 34;                       // 272-byte rows: a warp's 4-8 rows start in distinct banks
+constexpr int kTcTwBytes = 32 * kTcTwLd * 8;
+constexpr int kTcSmem = kTcTw + kTcTwBytes;
+static_assert(kTcFwdBHi % 16 == 0 && kTcTw % 16 == 0, "bulk-copy / descriptor bases must be 16-byte aligned");
 
-// Both DFT32 GEMMs of a 1024-point four-step transform of the 8 lines whose step-A
-// operand (rows (line, n1), K = n2) is already in the A planes, scaled by `scale`.
-// On return, warp w (line w) thread `lane` (k2) holds X[k2 + 32 k1] in x[k1]
-// (unscaled).  `tmem` holds 128 columns; `phase` is the barrier's next parity
-// (two phases are consumed).
-// NBLK = 2: 8 lines (all warps hold a line); NBLK = 1: 4 lines (warps 0-3), the
-// other warps only join the barriers.  bhi/blo: byte offsets of the DFT32 planes.
-template <int SIGN, int NBLK = 2>
+// Global table (built once per solver by k_tc_tables, same byte layout as shared memory):
+// [inverse DFT32 hi | lo][forward DFT32 hi | lo][twiddle matrix]
+constexpr int kTabInv = 0;
+constexpr int kTabFwd = 2 * kBBytes;
+constexpr int kTabTw = 4 * kBBytes;
+constexpr int kTabBytes = kTabTw + kTcTwBytes;
+
+__global__ void k_tc_tables(char* tab, const float2* __restrict__ tw1024) {
+  build_dft32<+1>(tab + kTabInv, tab + kTabInv + kBBytes, tw1024);
+  build_dft32<-1>(tab + kTabFwd, tab + kTabFwd + kBBytes, tw1024);
+  float2* t = reinterpret_cast<float2*>(tab + kTabTw);
+  for (int e = threadIdx.x; e < 32 * kTcTwLd; e += blockDim.x) {
+    const int n1 = e / kTcTwLd, k2 = e - n1 * kTcTwLd;
+    t[e] = k2 < 32 ? tw1024[(n1 * k2) & 1023] : make_float2(0.f, 0.f);
+  }
+}
+
+struct TcMisc {
+  uint64_t* bar;     // GEMM completion
+  uint32_t* tslot;
+  float* red;        // [8] per-warp maxima
+  uint64_t* setup;   // table bulk copies
+};
+__device__ __forceinline__ TcMisc tc_misc(char* sm) {
+  return {reinterpret_cast<uint64_t*>(sm + kTcMisc), reinterpret_cast<uint32_t*>(sm + kTcMisc + 8),
+          reinterpret_cast<float*>(sm + kTcMisc + 16), reinterpret_cast<uint64_t*>(sm + kTcMisc + 48)};
+}
+
+// One-time CTA setup: TMEM (128 columns), mbarriers, and TMA bulk copies of the DFT32
+// planes of the signs used plus the twiddle matrix.  The barriers are visible to the
+// other threads after the caller's next __syncthreads; tc_wait_tables before the
+// first GEMM.
+template <bool INV, bool FWD>
+__device__ __forceinline__ void tc_setup(char* sm, const TcMisc& m, const char* __restrict__ tab) {
+  if ((threadIdx.x >> 5) == 0) {
+    tmem_alloc(m.tslot, 128);
+    tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(m.bar, 1);
+    mbar_init(m.setup, 1);
+    mbar_fence_init();
+    constexpr uint32_t bytes = (INV ? 2 * kBBytes : 0) + (FWD ? 2 * kBBytes : 0) + kTcTwBytes;
+    mbar_arrive_expect_tx(m.setup, bytes);
+    if (INV) bulk_g2s(sm + kTcBHi, tab + kTabInv, 2 * kBBytes, m.setup);
+    if (FWD) bulk_g2s(sm + kTcFwdBHi, tab + kTabFwd, 2 * kBBytes + kTcTwBytes, m.setup);   // with the twiddles
+    else bulk_g2s(sm + kTcTw, tab + kTabTw, kTcTwBytes, m.setup);
+  }
+}
+__device__ __forceinline__ void tc_wait_tables(const TcMisc& m, int* err) { mbar_wait_bounded(m.setup, 0u, err, 4); }
+
+// warp maximum into red[warp]; after a __syncthreads every thread reads the CTA max
+__device__ __forceinline__ void warp_max_slot(float v, float* red) {
+  v = warp_max(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+}
+__device__ __forceinline__ float cta_max_slots(const float* red) {
+  float m = red[0];
+#pragma unroll
+  for (int i = 1; i < kTcThreads / 32; ++i) m = fmaxf(m, red[i]);
+  return m;
+}
+
+__device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+// four consecutive complex K values (one 16-byte core-matrix row) of operand row r,
+// starting at complex index 4*kc, scaled by s, split into the hi and lo planes
+__device__ __forceinline__ void put_c4(char* hi_plane, char* lo_plane, int r, int kc, float2 a, float2 b, float2 c,
+                                       float2 d, float s) {
+  __half2 h0, h1, h2, h3, l0, l1, l2, l3;
+  split2(a.x * s, a.y * s, h0, l0);
+  split2(b.x * s, b.y * s, h1, l1);
+  split2(c.x * s, c.y * s, h2, l2);
+  split2(d.x * s, d.y * s, h3, l3);
+  const uint32_t o = op_off(r, 8 * kc);
+  *reinterpret_cast<uint4*>(hi_plane + o) = make_uint4(h2bits(h0), h2bits(h1), h2bits(h2), h2bits(h3));
+  *reinterpret_cast<uint4*>(lo_plane + o) = make_uint4(h2bits(l0), h2bits(l1), h2bits(l2), h2bits(l3));
+}
+
+// Geometry of an L-line transform on 8 warps (L = 8: two M = 128 blocks, warp w reads
+// block w / 4 whole; L = 4: one block, warps w and w + 4 read its columns 0-31 / 32-63).
+// After either GEMM, thread (warp w, lane) owns TMEM row r = 128 blk + 32 (w & 3) + lane,
+// i.e. fixed index r / L of line r % L, and NC = 16 * L / 4 complex columns from `col0`.
+template <int L> struct TcGeom {
+  static_assert(L == 4 || L == 8, "4 or 8 lines");
+  static constexpr int NB = L / 4;                // M = 128 blocks
+  static constexpr int NC = 16 * NB;              // complex columns a thread reads
+  __device__ __forceinline__ static int row() {
+    const int w = threadIdx.x >> 5;
+    return (NB == 2 ? 128 * (w >> 2) : 0) + 32 * (w & 3) + (threadIdx.x & 31);
+  }
+  __device__ __forceinline__ static int line() { return row() % L; }
+  __device__ __forceinline__ static int index() { return row() / L; }
+  __device__ __forceinline__ static int col0() { return NB == 2 ? 0 : 16 * (int)(threadIdx.x >> 7); }
+  __device__ __forceinline__ static uint32_t taddr(uint32_t tmem) {
+    const int w = threadIdx.x >> 5;
+    return tmem + ((uint32_t)(32 * (w & 3)) << 16) + (NB == 2 ? (uint32_t)(64 * (w >> 2)) : (uint32_t)(32 * (w >> 2)));
+  }
+};
+
+template <int NC>
+__device__ __forceinline__ void tmem_read(uint32_t addr, float (&y)[2 * NC]) {
+#pragma unroll
+  for (int c = 0; c < (2 * NC) / 16; ++c) {
+    float v[16];
+    tmem_ld16(addr + 16 * c, v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) y[16 * c + i] = v[i];
+  }
+  tmem_wait_ld();
+}
+
+__device__ __forceinline__ void issue_blocks(int nb, uint32_t tmem, uint32_t base, int bhi, int blo) {
+  issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
+  if (nb == 2)
+    issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
+}
+
+// Both DFT32 GEMMs of the 1024-point four-step transform of L lines whose step-A
+// operand (row n1 * L + line, K = n2: x[n1 + 32 n2] * scale) the caller has written.
+// On return the thread's TcGeom row is (k2 = index, line) and x[j] = X[k2 + 32 (col0 + j)],
+// unscaled.  The barrier's next parity is `phase`; two phases are consumed.
+template <int SIGN, int L>
 __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t* bar, uint32_t phase, float scale,
-                                              const float2* __restrict__ tw, int* err, float2 (&x)[32],
-                                              int bhi = kTcBHi, int blo = kTcBLo) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int blk = warp >> 2, quad = warp & 3;
-  const bool active = blk < NBLK;
-  unsigned* maxw = reinterpret_cast<unsigned*>(sm + kTcMisc + 12);
+                                              int* err, float2 (&x)[TcGeom<L>::NC]) {
+  using G = TcGeom<L>;
+  constexpr int NC = G::NC;
+  const int bhi = SIGN > 0 ? kTcBHi : kTcFwdBHi, blo = SIGN > 0 ? kTcBLo : kTcFwdBLo;
   const uint32_t base = smem_u32(sm);
-  // ---- step A: DFT32 over n2 for every row (line, n1)
+  // ---- step A: DFT32 over n2 for every row (n1, line)
   fence_proxy_async();
   fence_before_sync();
   __syncthreads();
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     fence_after_sync();
-    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
-    if (NBLK == 2)
-      issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
+    issue_blocks(G::NB, tmem, base, bhi, blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase, err, 2);
   fence_after_sync();
-  // row (line = warp, n1 = lane): Y[n1][k2] for k2 = 0..31 in columns 64*blk + 2k2 (+1)
-  float y[64];
-  const uint32_t lane_base = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(64 * blk);
-  if (active) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      float v[16];
-      tmem_ld16(lane_base + 16 * c, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) y[16 * c + i] = v[i];
-    }
-    tmem_wait_ld();
-  } else {
-#pragma unroll
-    for (int i = 0; i < 64; ++i) y[i] = 0.f;
-  }
-  // twiddle W_1024^{SIGN n1 k2}
-  float mx = 0.f;
-#pragma unroll
-  for (int k2 = 0; k2 < 32; ++k2) {
-    float2 w = __ldg(tw + ((lane * k2) & 1023));
-    if (SIGN > 0) w.y = -w.y;
-    const float re = y[2 * k2] * w.x - y[2 * k2 + 1] * w.y;
-    const float im = y[2 * k2] * w.y + y[2 * k2 + 1] * w.x;
-    y[2 * k2] = re;
-    y[2 * k2 + 1] = im;
-    mx = fmaxf(mx, fmaxf(fabsf(re), fabsf(im)));
-  }
-  const float scale2 = pow2_scale(cta_max(mx, maxw));
-  fence_before_sync();
-  __syncthreads();   // every warp has read its accumulator before step C overwrites it
-  // ---- step C operand: rows (line, k2), K = n1 (this thread's lane)
+  float y[2 * NC];
+  tmem_read<NC>(G::taddr(tmem), y);
+  const int n1 = G::index(), line = G::line(), c0 = G::col0();
+  // twiddle W_1024^{SIGN n1 k2}; step-C operand rows (k2, line), K = n1, at scale 2^-5
+  // (the step-A GEMM has completed, so its operand planes are free; the accumulator is
+  // only overwritten by the step-C GEMM, issued after every thread's TMEM read)
   char* a_hi = sm + kTcAHi;
   char* a_lo = sm + kTcALo;
-  if (active) {
+  const float4* trow = reinterpret_cast<const float4*>(sm + kTcTw + n1 * kTcTwLd * 8) + c0 / 2;
 #pragma unroll
-    for (int k2 = 0; k2 < 32; ++k2)
-      put_c(a_hi, a_lo, warp * 32 + k2, lane, y[2 * k2] * scale2, y[2 * k2 + 1] * scale2);
+  for (int j = 0; j < NC; j += 2) {
+    const float4 t4 = trow[j / 2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int k2 = c0 + j + e;
+      const float wx = e ? t4.z : t4.x, wy = SIGN > 0 ? -(e ? t4.w : t4.y) : (e ? t4.w : t4.y);
+      const float re = (y[2 * (j + e)] * wx - y[2 * (j + e) + 1] * wy) * 0.03125f;
+      const float im = (y[2 * (j + e)] * wy + y[2 * (j + e) + 1] * wx) * 0.03125f;
+      put_c(a_hi, a_lo, k2 * L + line, n1, re, im);
+    }
   }
   fence_proxy_async();
   fence_before_sync();
   __syncthreads();
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     fence_after_sync();
-    issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
-    if (NBLK == 2)
-      issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
+    issue_blocks(G::NB, tmem, base, bhi, blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase ^ 1u, err, 3);
   fence_after_sync();
-  // row (line = warp, k2 = lane): X[k2 + 32 k1] in columns 64*blk + 2k1 (+1)
-  const float inv = 1.f / (scale * scale2);   // exact: both are powers of two
-  if (active) {
+  tmem_read<NC>(G::taddr(tmem), y);
+  const float inv = 32.f / scale;   // exact: powers of two
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      float v[16];
-      tmem_ld16(lane_base + 16 * c, v);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) x[8 * c + i] = make_float2(v[2 * i] * inv, v[2 * i + 1] * inv);
-    }
-    tmem_wait_ld();
+  for (int j = 0; j < NC; ++j) x[j] = make_float2(y[2 * j] * inv, y[2 * j + 1] * inv);
+}
+
+__device__ __forceinline__ void tc_teardown(uint32_t tmem) {
+  fence_before_sync();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) {
+    fence_after_sync();
+    tmem_dealloc(tmem, 128);
   }
 }
 
+// ---------------------------------------------------------------------------------------
 // Standalone 2D-FFT pass over 8 lines of a 1024 x 1024 field: AXIS 0 = rows
 // (contiguous), AXIS 1 = columns.  Forward unscaled, inverse scaled 1/N per pass,
 // as the FP32 passes (fft.js:58-59).
+constexpr int kTcLines = 8;
+constexpr int kTcRowLd = 1024 + 4;                // padded staging line (rows pass)
+static_assert(kTcLines * kTcRowLd * 8 <= kTcMisc, "row staging must fit below the misc words");
+
 template <int AXIS, int SIGN>
-__global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const float2* __restrict__ tw, int* err) {
+__global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const char* __restrict__ tab, int* err) {
   constexpr int N = 1024;
   extern __shared__ __align__(1024) char sm[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTcMisc);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 8);
-  unsigned* maxw = reinterpret_cast<unsigned*>(sm + kTcMisc + 12);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TcMisc m = tc_misc(sm);
+  const int tid = threadIdx.x;
   const int l0 = blockIdx.x * kTcLines;
-  if (warp == 0) {
-    tmem_alloc(tslot, 128);
-    tmem_relinquish();
-  }
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-  }
-  build_dft32<SIGN>(sm + kTcBHi, sm + kTcBLo, tw);
-  // load: thread (line g, n1 t) takes x[t + 32 n2] for n2 = 0..31 -- one whole operand row
-  const int g = AXIS == 0 ? warp : (tid & 7), t = AXIS == 0 ? lane : (tid >> 3);
+  // load: thread (line g, n1 t) takes x[t + 32 n2], n2 = 0..31 -- one whole operand row
+  const int g = tid & 7, t = tid >> 3;
   float2 v[32];
   float mx = 0.f;
 #pragma unroll
@@ -311,86 +404,74 @@ __global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const float
     v[n2] = AXIS == 0 ? data[(size_t)(l0 + g) * N + y] : data[(size_t)y * N + l0 + g];
     mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
   }
-  const float scale = pow2_scale(cta_max(mx, maxw));
-#pragma unroll
-  for (int n2 = 0; n2 < 32; ++n2) put_c(sm + kTcAHi, sm + kTcALo, g * 32 + t, n2, v[n2].x * scale, v[n2].y * scale);
-  __syncthreads();   // the TMEM address written by warp 0 is visible to all
-  const uint32_t tmem = *tslot;
-  float2 x[32];
-  fft1024_gemms<SIGN>(sm, tmem, bar, 0u, scale, tw, err, x);
-  const float post = SIGN > 0 ? 1.f / N : 1.f;
-  // stage through shared memory (over the operands, no longer read) for coalesced stores
-  float2* st = reinterpret_cast<float2*>(sm);
+  tc_setup<(SIGN > 0), (SIGN < 0)>(sm, m, tab);
+  warp_max_slot(mx, m.red);
   __syncthreads();
+  const float scale = pow2_scale(cta_max_slots(m.red));
+  const uint32_t tmem = *m.tslot;
+#pragma unroll
+  for (int kc = 0; kc < 8; ++kc)
+    put_c4(sm + kTcAHi, sm + kTcALo, t * kTcLines + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3],
+           scale);
+  tc_wait_tables(m, err);
+  float2 x[32];
+  fft1024_gemms<SIGN, 8>(sm, tmem, m.bar, 0u, scale, err, x);
+  const float post = SIGN > 0 ? 1.f / N : 1.f;
+  // thread: line = lane & 7, k2; X[k2 + 32 k1] in x[k1].  Stage (over the dead operands)
+  // for coalesced stores.
+  // (both GEMMs have completed: operand and DFT planes are free)
+  using G = TcGeom<8>;
+  const int line = G::line(), k2 = G::index();
+  float2* st = reinterpret_cast<float2*>(sm);
 #pragma unroll
   for (int k1 = 0; k1 < 32; ++k1) {
-    const int y = lane + 32 * k1;
-    if (AXIS == 0) st[warp * (N + 1) + y] = make_float2(x[k1].x * post, x[k1].y * post);
-    else st[y * kTcStageLd + warp] = make_float2(x[k1].x * post, x[k1].y * post);
+    const int y = k2 + 32 * k1;
+    const float2 o = make_float2(x[k1].x * post, x[k1].y * post);
+    if (AXIS == 0) st[line * kTcRowLd + y] = o;
+    else st[y * kTcLines + line] = o;
   }
   __syncthreads();
 #pragma unroll 4
   for (int i = tid; i < kTcLines * N; i += kTcThreads) {
     if (AXIS == 0) {
-      const int gl = i / N, y = i - gl * N;
-      data[(size_t)(l0 + gl) * N + y] = st[gl * (N + 1) + y];
+      const int gl = i >> 10, y = i & (N - 1);
+      data[(size_t)(l0 + gl) * N + y] = st[gl * kTcRowLd + y];
     } else {
-      const int y = i >> 3, gl = i & 7;
-      data[(size_t)y * N + l0 + gl] = st[y * kTcStageLd + gl];
+      data[(size_t)(i >> 3) * N + l0 + (i & 7)] = st[i];
     }
   }
-  fence_before_sync();
-  __syncthreads();
-  if (warp == 0) {
-    fence_after_sync();
-    tmem_dealloc(tmem, 128);
-  }
+  tc_teardown(tmem);
 }
 
 // ---------------------------------------------------------------------------------------
 // Fused physical-column stage at 1024^2 with both y-transforms on the tensor cores
 // (the tcgen05 counterpart of k_phys_cols): a CTA owns 4 columns x0..x0+3.
-//   lines 0-3 = PA columns, 4-7 = PB columns -> one 8-line inverse transform
-//   warps 4-7 hand v(y) to warps 0-3 through shared memory
-//   warps 0-3 form (u omega, v omega) -> one 4-line forward transform -> in-band Z rows
+//   lines 0-3 = PA columns, 4-7 = PB columns -> one 8-line inverse transform; the PA
+//   and PB lines of a column then sit 4 lanes apart in one warp (shuffle exchange)
+//   (u omega, v omega) of the 4 columns -> one 4-line forward transform -> in-band Z rows
 // MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage (+ velocity, speed).
-// Shared memory after the inverse transform (the operands are dead once its second
-// GEMM has completed): v exchange over the block-1 hi plane, (u, v) staging over the
-// block-1 lo plane and the inverse DFT32 planes, forward operands in block 0, Z
-// staging over block 0.
+// Shared memory after the inverse transform: the (u, v) staging tile over the block-1
+// operand planes (y < 512 in the hi plane, y >= 512 in the lo plane), the forward
+// operands in block 0, the Z staging tile over block 0 once the GEMMs are done.
 constexpr int kTcCols = 4;
 constexpr int kTcColsGrid = 1024 / kTcCols;
-constexpr int kTcColsBHi = kTcSmem;                      // forward DFT32 planes, after the misc words
-constexpr int kTcColsBLo = kTcSmem + kBBytes;
-constexpr int kTcColsSmem = kTcSmem + 2 * kBBytes;
-constexpr int kTcColsExch = kBlockBytes;                 // float [4][1024]
-constexpr int kTcColsVel = 3 * kBlockBytes;              // float2 [1024][4], up to kTcMisc
-static_assert(kTcColsVel + 1024 * kTcCols * 8 <= kTcMisc, "velocity staging overlaps the misc words");
-static_assert(kTcColsBHi % 16 == 0, "descriptor base must be 16-byte aligned");
+constexpr int kTcColsSmem = kTcSmem;
 
-// (y, col) -> float2 slot of a [1024][4] staging tile; the XOR spreads a warp's
-// fixed-column, consecutive-y writes over all banks
+// (y, col) -> float2 slot of a [1024][4] staging tile; the XOR spreads a warp's writes
+// (4 columns x 8 consecutive y) over all banks
 __device__ __forceinline__ int cols_stage_idx(int y, int col) { return 4 * y + (col ^ ((y >> 2) & 3)); }
+__device__ __forceinline__ float2* vel_stage_slot(char* sm, int y, int col) {
+  char* base = sm + (y < 512 ? kTcAHi + kBlockBytes : kTcALo + kBlockBytes);
+  return reinterpret_cast<float2*>(base) + cols_stage_idx(y & 511, col);
+}
 
 template <int MODE>
-__global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, int* err) {
+__global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, const char* __restrict__ tab, int* err) {
   constexpr int N = 1024;
   extern __shared__ __align__(1024) char sm[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTcMisc);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 8);
-  unsigned* maxw = reinterpret_cast<unsigned*>(sm + kTcMisc + 12);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TcMisc m = tc_misc(sm);
+  const int tid = threadIdx.x, lane = tid & 31;
   const int x0 = blockIdx.x * kTcCols;
-  if (warp == 0) {
-    tmem_alloc(tslot, 128);
-    tmem_relinquish();
-  }
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-  }
-  build_dft32<+1>(sm + kTcBHi, sm + kTcBLo, a.tw);
-  if (MODE != 0) build_dft32<-1>(sm + kTcColsBHi, sm + kTcColsBLo, a.tw);
   // load: thread (line g, n1 t) takes the pack at ky = t + 32 n2 -- one operand row
   const int g = tid & 7, t = tid >> 3;
   const float2* src = (g < kTcCols ? a.pa : a.pb) + x0 + (g & (kTcCols - 1));
@@ -401,77 +482,69 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, int*
     v[n2] = __ldcs(src + (size_t)(t + 32 * n2) * N);
     mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
   }
-  const float scale = pow2_scale(cta_max(mx, maxw));
-#pragma unroll
-  for (int n2 = 0; n2 < 32; ++n2) put_c(sm + kTcAHi, sm + kTcALo, g * 32 + t, n2, v[n2].x * scale, v[n2].y * scale);
-  __syncthreads();   // the TMEM address written by warp 0 is visible to all
-  const uint32_t tmem = *tslot;
-  float2 x[32];
-  fft1024_gemms<+1, 2>(sm, tmem, bar, 0u, scale, a.tw, err, x);
-  // warp w < 4: (omega, u) of column x0 + w at y = lane + 32 k1; warp 4 + w: (v, 0)
-  float* sv = reinterpret_cast<float*>(sm + kTcColsExch);
-  if (warp >= kTcCols) {
-#pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) sv[(warp - kTcCols) * N + lane + 32 * k1] = x[k1].x;
-  }
+  tc_setup<true, MODE != 0>(sm, m, tab);
+  warp_max_slot(mx, m.red);
   __syncthreads();
-  float speed = 0.f, mz = 0.f;
-  float2* svel = reinterpret_cast<float2*>(sm + kTcColsVel);
-  if (warp < kTcCols) {
+  const float scale = pow2_scale(cta_max_slots(m.red));
+  const uint32_t tmem = *m.tslot;
 #pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) {
-      const int y = lane + 32 * k1;
-      const float om = x[k1].x, u = x[k1].y, w = sv[warp * N + y];
-      if (MODE != 1) {
-        svel[cols_stage_idx(y, warp)] = make_float2(u, w);
-        speed = fmaxf(speed, fabsf(u) + fabsf(w));
-      }
-      x[k1] = make_float2(u * om, w * om);
-      mz = fmaxf(mz, fmaxf(fabsf(x[k1].x), fabsf(x[k1].y)));
+  for (int kc = 0; kc < 8; ++kc)
+    put_c4(sm + kTcAHi, sm + kTcALo, t * 8 + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3], scale);
+  tc_wait_tables(m, err);
+  float2 x[32];
+  fft1024_gemms<+1, 8>(sm, tmem, m.bar, 0u, scale, err, x);
+  // thread: line = lane & 7 (PA column c = line & 3 for line < 4, PB column for line >= 4),
+  // k2 = TcGeom<8>::index(); x[k1] at y = k2 + 32 k1.  The partner line is lane ^ 4.
+  const bool is_pa = (lane & 4) == 0;
+  const int c = lane & 3, k2 = TcGeom<8>::index();
+  float speed = 0.f, mz = 0.f;
+#pragma unroll
+  for (int k1 = 0; k1 < 32; ++k1) {
+    const float px = __shfl_xor_sync(0xffffffffu, x[k1].x, 4);
+    const float py = __shfl_xor_sync(0xffffffffu, x[k1].y, 4);
+    const float om = is_pa ? x[k1].x : px, u = is_pa ? x[k1].y : py, w = is_pa ? px : x[k1].x;
+    if (MODE != 1 && is_pa) {
+      *vel_stage_slot(sm, k2 + 32 * k1, c) = make_float2(u, w);
+      speed = fmaxf(speed, fabsf(u) + fabsf(w));
+    }
+    x[k1] = make_float2(u * om, w * om);
+    mz = fmaxf(mz, fmaxf(fabsf(x[k1].x), fabsf(x[k1].y)));
+  }
+  if (MODE != 0) warp_max_slot(mz, m.red);
+  __syncthreads();   // staged velocity and the product maxima are visible
+  if (MODE != 1) {
+#pragma unroll 4
+    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
+      const int y = i >> 2, cc = i & 3;
+      a.vel[(size_t)y * N + x0 + cc] = *vel_stage_slot(sm, y, cc);
     }
   }
   if (MODE != 0) {
-    const float scale_z = pow2_scale(cta_max(mz, maxw));   // its barriers also publish svel
-    if (MODE == 2) {
-#pragma unroll 4
-      for (int i = tid; i < N * kTcCols; i += kTcThreads) {
-        const int y = i >> 2, c = i & 3;
-        a.vel[(size_t)y * N + x0 + c] = svel[cols_stage_idx(y, c)];
-      }
-    }
-    // forward operand: rows (line = warp, n1 = lane), K = n2 = k1 (block 0 only)
-    if (warp < kTcCols) {
+    const float scale_z = pow2_scale(cta_max_slots(m.red));
+    // forward operand: row (n1 = k2, c), K = n2 = k1; the PA lane writes k1 0-15, its
+    // PB partner (same products) k1 16-31
 #pragma unroll
-      for (int k1 = 0; k1 < 32; ++k1)
-        put_c(sm + kTcAHi, sm + kTcALo, warp * 32 + lane, k1, x[k1].x * scale_z, x[k1].y * scale_z);
+    for (int q = 0; q < 4; ++q) {
+      const float2 z0 = is_pa ? x[4 * q] : x[16 + 4 * q], z1 = is_pa ? x[4 * q + 1] : x[16 + 4 * q + 1];
+      const float2 z2 = is_pa ? x[4 * q + 2] : x[16 + 4 * q + 2], z3 = is_pa ? x[4 * q + 3] : x[16 + 4 * q + 3];
+      put_c4(sm + kTcAHi, sm + kTcALo, k2 * 4 + c, is_pa ? q : 4 + q, z0, z1, z2, z3, scale_z);
     }
-    fft1024_gemms<-1, 1>(sm, tmem, bar, 0u, scale_z, a.tw, err, x, kTcColsBHi, kTcColsBLo);
-    // warp w < 4: Z(ky = lane + 32 k1, x0 + w); stage for row-contiguous stores of the in-band rows
-    float2* sz = reinterpret_cast<float2*>(sm);
-    if (warp < kTcCols) {
+    float2 zf[16];
+    fft1024_gemms<-1, 4>(sm, tmem, m.bar, 0u, scale_z, err, zf);
+    // thread: column c' = lane & 3, k2' = TcGeom<4>::index(); Z(ky = k2' + 32 (col0 + j))
+    using G4 = TcGeom<4>;
+    const int cz = G4::line(), kz = G4::index(), c0 = G4::col0();
+    float2* sz = reinterpret_cast<float2*>(sm);   // over the dead operands
 #pragma unroll
-      for (int k1 = 0; k1 < 32; ++k1) sz[cols_stage_idx(lane + 32 * k1, warp)] = x[k1];
-    }
+    for (int j = 0; j < 16; ++j) sz[cols_stage_idx(kz + 32 * (c0 + j), cz)] = zf[j];
     __syncthreads();
 #pragma unroll 4
     for (int i = tid; i < N * kTcCols; i += kTcThreads) {
-      const int row = i >> 2, c = i & 3;
-      if (fabsf(wn<N>(row)) < Tune<N>::KCUT) a.z[(size_t)row * N + x0 + c] = sz[cols_stage_idx(row, c)];
-    }
-  } else {
-    __syncthreads();
-#pragma unroll 4
-    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
-      const int y = i >> 2, c = i & 3;
-      a.vel[(size_t)y * N + x0 + c] = svel[cols_stage_idx(y, c)];
+      const int row = i >> 2, cc = i & 3;
+      if (fabsf(wn<N>(row)) < Tune<N>::KCUT) a.z[(size_t)row * N + x0 + cc] = sz[cols_stage_idx(row, cc)];
     }
   }
-  fence_before_sync();
-  __syncthreads();
-  if (warp == 0) {
-    fence_after_sync();
-    tmem_dealloc(tmem, 128);
-  }
+  tc_teardown(tmem);
   if (MODE != 1) cols_speed_finalize<kTcThreads>(a, speed);
 }
 
