@@ -16,7 +16,9 @@
 //     dyeScale 2.  A sample outside the on-chip region is recomputed from global
 //     memory (the forward/backward values at that texel are re-derived), so the
 //     result does not depend on the halo being large enough.  Texture traffic
-//     drops from 7 texture passes to one read and one write.
+//     drops from 7 texture passes to one read and one write.  The windows hold
+//     the texels as the binary16 values the textures would hold (exact), and only
+//     r, g, b are carried: the corrected texel's alpha is 1 whatever the inputs.
 #pragma once
 #include <cuda_fp16.h>
 #include "s2d_device.cuh"
@@ -206,31 +208,39 @@ constexpr int kDyeW3 = kDyeTile + 6 * kDyeHalo;   // source region edge
 // under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
 __host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
 __host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
-  return sizeof(float4) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
-         sizeof(float2) * (2 * kDyeW2 * kDyeW2 + dye_vel_edge(n, m) * dye_vel_edge(n, m));
+  return sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
+         sizeof(float2) * (kDyeW2 * kDyeW2 + kDyeTile * kDyeTile + dye_vel_edge(n, m) * dye_vel_edge(n, m));
 }
 
-__device__ __forceinline__ Rgba from4(float4 v) { return {v.x, v.y, v.z, v.w}; }
+struct Rgb {
+  float r, g, b;
+};
+__device__ __forceinline__ Rgb rgb_of(uint2 u) {
+  const float2 rg = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  return {rg.x, rg.y, __low2float(*reinterpret_cast<const __half2*>(&u.y))};
+}
+// binary16 texel (r, g, b, alpha 1) of FP32 channels, as a texture store rounds them
+__device__ __forceinline__ uint2 pack_rgb(const Rgb& c) { return pack_texel(c.r, c.g, c.b, 1.f); }
 
-// on-chip window of FP32 texels with an exact global fallback (coordinates are wrapped indices)
+// on-chip window of binary16 texels with an exact global fallback (coordinates are wrapped indices)
 struct SmemTex {
-  const float4* sm;
+  const uint2* sm;
   int ox, oy, w, m;
   const uint2* g;
-  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+  __device__ __forceinline__ uint2 operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
-    return unpack_texel(__ldg(g + (size_t)y * m + x));
+    if (rx < w && ry < w) return sm[ry * w + rx];
+    return __ldg(g + (size_t)y * m + x);
   }
   // the 2x2 footprint in one window test (slots rx, rx+1 hold texels x0, x1 = x0+1 wrapped)
-  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
+  __device__ __forceinline__ bool quad(const Footprint& f, uint2 (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
     if (rx + 1 < w && ry + 1 < w) {
-      const float4* p = sm + ry * w + rx;
-      c00 = from4(p[0]);
-      c10 = from4(p[1]);
-      c01 = from4(p[w]);
-      c11 = from4(p[w + 1]);
+      const uint2* p = sm + ry * w + rx;
+      c[0] = p[0];
+      c[1] = p[1];
+      c[2] = p[w];
+      c[3] = p[w + 1];
       return true;
     }
     return false;
@@ -280,15 +290,18 @@ __device__ __forceinline__ float2 sample_vel(const WinVel& w, float px, float py
   return sample_vel_win(w.v, px, py);
 }
 
+// r, g, b of the bilinear sample over a footprint, optionally with the 4-texel min / max
+// (the same per-channel arithmetic as bilerp)
 template <class TF>
-__device__ __forceinline__ Rgba bilerp_win(const TF& tf, const Footprint& f, Rgba* lo = nullptr, Rgba* hi = nullptr) {
-  Rgba c00, c10, c01, c11;
-  if (!tf.quad(f, c00, c10, c01, c11)) {
-    c00 = tf(f.x0, f.y0);
-    c10 = tf(f.x1, f.y0);
-    c01 = tf(f.x0, f.y1);
-    c11 = tf(f.x1, f.y1);
+__device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) {
+  uint2 q[4];
+  if (!tf.quad(f, q)) {
+    q[0] = tf(f.x0, f.y0);
+    q[1] = tf(f.x1, f.y0);
+    q[2] = tf(f.x0, f.y1);
+    q[3] = tf(f.x1, f.y1);
   }
+  const Rgb c00 = rgb_of(q[0]), c10 = rgb_of(q[1]), c01 = rgb_of(q[2]), c11 = rgb_of(q[3]);
   if (lo) {
     lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
     lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
@@ -298,92 +311,79 @@ __device__ __forceinline__ Rgba bilerp_win(const TF& tf, const Footprint& f, Rgb
     hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
   }
   return {lerp2(c00.r, c10.r, c01.r, c11.r, f.fx, f.fy), lerp2(c00.g, c10.g, c01.g, c11.g, f.fx, f.fy),
-          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
+          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy)};
 }
 
-// forward-pass value at texel (x, y), as the advect_fwd texture would hold it
+// binary16 window whose texels outside the window are re-derived by EVAL
+template <class EVAL>
+struct DerivedTex {
+  const uint2* sm;
+  int ox, oy, w, m;
+  const EVAL& eval;
+  __device__ __forceinline__ uint2 operator()(int x, int y) const {
+    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
+    if (rx < w && ry < w) return sm[ry * w + rx];
+    return eval(x, y);
+  }
+  __device__ __forceinline__ bool quad(const Footprint& f, uint2 (&c)[4]) const {
+    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
+    if (rx + 1 < w && ry + 1 < w) {
+      const uint2* p = sm + ry * w + rx;
+      c[0] = p[0];
+      c[1] = p[1];
+      c[2] = p[w];
+      c[3] = p[w + 1];
+      return true;
+    }
+    return false;
+  }
+};
+
+// forward-pass texel (x, y) as the advect_fwd texture would hold it
 struct FwdEval {
   const SmemVel& vel;
   const SmemTex& src;
   float h;
   int n, m;
-  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+  __device__ __forceinline__ uint2 operator()(int x, int y) const {
     const float2 p = texel_pos(x, y, m);
     const float2 s = trace_from(WinVel{vel}, p.x, p.y, sample_vel_win(vel, p.x, p.y), h, n);
-    return round_texel(bilerp_win(src, footprint(s.x, s.y, m)));
+    return pack_rgb(bilerp_rgb(src, footprint(s.x, s.y, m)));
   }
 };
-// forward values: on-chip window, else recomputed
-struct FwdFetch {
-  const float4* sm;
-  int ox, oy, w, m;
-  const FwdEval& eval;
-  __device__ __forceinline__ Rgba operator()(int x, int y) const {
-    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
-    return eval(x, y);
-  }
-  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
-    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
-    if (rx + 1 < w && ry + 1 < w) {
-      const float4* p = sm + ry * w + rx;
-      c00 = from4(p[0]);
-      c10 = from4(p[1]);
-      c01 = from4(p[w]);
-      c11 = from4(p[w + 1]);
-      return true;
-    }
-    return false;
-  }
-};
-// backward-pass value at texel (x, y), as the advect_back texture would hold it
+using FwdFetch = DerivedTex<FwdEval>;
+// backward-pass texel (x, y) as the advect_back texture would hold it
 struct BackEval {
   const SmemVel& vel;
   const FwdFetch& fwd;
   float h;
   int n, m;
-  __device__ __forceinline__ Rgba operator()(int x, int y) const {
+  __device__ __forceinline__ uint2 operator()(int x, int y) const {
     const float2 p = texel_pos(x, y, m);
     const float2 s = trace_from(WinVel{vel}, p.x, p.y, sample_vel_win(vel, p.x, p.y), -h, n);
-    return round_texel(bilerp_win(fwd, footprint(s.x, s.y, m)));
+    return pack_rgb(bilerp_rgb(fwd, footprint(s.x, s.y, m)));
   }
 };
-struct BackFetch {
-  const float4* sm;
-  int ox, oy, w, m;
-  const BackEval& eval;
-  __device__ __forceinline__ Rgba operator()(int x, int y) const {
-    const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return from4(sm[ry * w + rx]);
-    return eval(x, y);
-  }
-  __device__ __forceinline__ bool quad(const Footprint& f, Rgba& c00, Rgba& c10, Rgba& c01, Rgba& c11) const {
-    const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
-    if (rx + 1 < w && ry + 1 < w) {
-      const float4* p = sm + ry * w + rx;
-      c00 = from4(p[0]);
-      c10 = from4(p[1]);
-      c01 = from4(p[w]);
-      c11 = from4(p[w + 1]);
-      return true;
-    }
-    return false;
-  }
-};
+using BackFetch = DerivedTex<BackEval>;
 
-__device__ __forceinline__ float4 to4(const Rgba& c) { return make_float4(c.r, c.g, c.b, c.a); }
+// BFECC correction from r, g, b (the arithmetic of correct_from; alpha is not read)
+__device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const Rgb& lo, const Rgb& hi, float px,
+                                             float py, float fade, const DevSplats* __restrict__ S) {
+  const Rgba a4{a.r, a.g, a.b, 1.f}, b4{b.r, b.g, b.b, 1.f}, lo4{lo.r, lo.g, lo.b, 0.f}, hi4{hi.r, hi.g, hi.b, 0.f};
+  return correct_from(a4, b4, lo4, hi4, px, py, fade, S);
+}
 
 __global__ void __launch_bounds__(kDyeThreads)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
                 const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
                 const DevSplats* __restrict__ S, int n, int m) {
-  extern __shared__ float4 dsm4[];
-  float4* s_back = dsm4;
-  float4* s_fwd = s_back + kDyeW1 * kDyeW1;
-  float4* s_src = s_fwd + kDyeW2 * kDyeW2;
+  extern __shared__ uint2 dsm2[];
+  uint2* s_back = dsm2;
+  uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
+  uint2* s_src = s_fwd + kDyeW2 * kDyeW2;
   float2* s_v1 = reinterpret_cast<float2*>(s_src + kDyeW3 * kDyeW3);   // velocity at forward-region texels
-  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // forward trace positions
-  float2* s_vel = s_sp + kDyeW2 * kDyeW2;
+  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // forward trace positions of the tile
+  float2* s_vel = s_sp + kDyeTile * kDyeTile;
   const int vw = dye_vel_edge(n, m);
   const int tx0 = blockIdx.x * kDyeTile, ty0 = blockIdx.y * kDyeTile;
   const int tid = threadIdx.x;
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kDyeThreads)
 #pragma unroll 4
   for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
     const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
-    s_src[i] = to4(unpack_texel(__ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)))));
+    s_src[i] = __ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
   }
 #pragma unroll 4
   for (int i = tid; i < vw * vw; i += kDyeThreads) {
@@ -419,13 +419,14 @@ __global__ void __launch_bounds__(kDyeThreads)
   }
   __syncthreads();
 
-  // forward pass over the forward region; keep its trace positions for the correction
+  // forward pass over the forward region; keep the tile's trace positions for the correction
   for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
     const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
     const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
     const float2 sp = trace_from(WinVel{V}, p.x, p.y, s_v1[i], h, n);
-    s_sp[i] = sp;
-    s_fwd[i] = to4(round_texel(bilerp_win(T, footprint(sp.x, sp.y, m))));
+    const int tx = rx - 2 * kDyeHalo, ty = ry - 2 * kDyeHalo;
+    if ((unsigned)tx < (unsigned)kDyeTile && (unsigned)ty < (unsigned)kDyeTile) s_sp[ty * kDyeTile + tx] = sp;
+    s_fwd[i] = pack_rgb(bilerp_rgb(T, footprint(sp.x, sp.y, m)));
   }
   __syncthreads();
 
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(kDyeThreads)
     const int fi = (ry + kDyeHalo) * kDyeW2 + rx + kDyeHalo;
     const float2 p = texel_pos((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1), m);
     const float2 sb = trace_from(WinVel{V}, p.x, p.y, s_v1[fi], -h, n);
-    s_back[i] = to4(round_texel(bilerp_win(ff, footprint(sb.x, sb.y, m))));
+    s_back[i] = pack_rgb(bilerp_rgb(ff, footprint(sb.x, sb.y, m)));
   }
   __syncthreads();
 
@@ -448,12 +449,12 @@ __global__ void __launch_bounds__(kDyeThreads)
     const int ry = i / kDyeTile, rx = i - ry * kDyeTile;
     const int x = tx0 + rx, y = ty0 + ry;
     const float2 p = texel_pos(x, y, m);
-    const float2 sp = s_sp[(ry + 2 * kDyeHalo) * kDyeW2 + rx + 2 * kDyeHalo];
+    const float2 sp = s_sp[i];
     const Footprint f = footprint(sp.x, sp.y, m);
-    Rgba lo, hi;
-    const Rgba a = bilerp_win(T, f, &lo, &hi);
-    const Rgba b = bilerp_win(bf, f);
-    dst[(size_t)y * m + x] = correct_from(a, b, lo, hi, p.x, p.y, fade, S);
+    Rgb lo, hi;
+    const Rgb a = bilerp_rgb(T, f, &lo, &hi);
+    const Rgb b = bilerp_rgb(bf, f);
+    dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, p.x, p.y, fade, S);
   }
 }
 
