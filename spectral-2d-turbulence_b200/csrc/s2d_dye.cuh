@@ -11,14 +11,15 @@
 //   * k_dye_fused: one launch per step.  A CTA owns a 32 x 32 output tile and
 //     keeps, in shared memory, the source texels of the tile plus a 3-level halo,
 //     the forward-pass texels of the tile plus 2 levels and the backward-pass
-//     texels plus 1 level; each level's halo (2 texels) covers the bilinear
-//     footprint of a back-trace of up to one texel, which the CFL limit gives at
-//     dyeScale 2.  A sample outside the on-chip region is recomputed from global
+//     texels plus 1 level; each level's halo (1 texel below, 2 above) covers the
+//     bilinear footprint of a back-trace of up to one texel, which the CFL limit
+//     gives at dyeScale 2.  A sample outside the on-chip region is recomputed from global
 //     memory (the forward/backward values at that texel are re-derived), so the
 //     result does not depend on the halo being large enough.  Texture traffic
-//     drops from 7 texture passes to one read and one write.  The windows hold
-//     the texels as the binary16 values the textures would hold (exact), and only
-//     r, g, b are carried: the corrected texel's alpha is 1 whatever the inputs.
+//     drops from 7 texture passes to one read and one write.  The forward and
+//     backward windows hold the binary16 values those textures would hold
+//     (exact), the source window their FP32 expansion, and only r, g, b are
+//     carried: the corrected texel's alpha is 1 whatever the inputs.
 #pragma once
 #include <cuda_fp16.h>
 #include "s2d_device.cuh"
@@ -198,17 +199,20 @@ __global__ void k_dye_correct(const float2* __restrict__ vel, const uint2* __res
 
 // ---------------------------------------------------------------- fused single pass
 constexpr int kDyeTile = 32;         // output tile edge
-constexpr int kDyeHalo = 2;          // halo per level (texels)
+// Halo per level: a sample displaced by at most one texel from texel x has the bilinear
+// footprint [x - 1, x + 2], so each level extends the region below by 1 and above by 2.
+constexpr int kDyeLo = 1, kDyeHi = 2;
 constexpr int kDyeThreads = 256;
-constexpr int kDyeW1 = kDyeTile + 2 * kDyeHalo;   // backward-pass region edge
-constexpr int kDyeW2 = kDyeTile + 4 * kDyeHalo;   // forward-pass region edge
-constexpr int kDyeW3 = kDyeTile + 6 * kDyeHalo;   // source region edge
+constexpr int kDyeW1 = kDyeTile + (kDyeLo + kDyeHi);       // backward-pass region edge
+constexpr int kDyeW2 = kDyeTile + 2 * (kDyeLo + kDyeHi);   // forward-pass region edge
+constexpr int kDyeW3 = kDyeTile + 3 * (kDyeLo + kDyeHi);   // source region edge
 
 // velocity cells needed by traces from the forward-pass region, for an n x n velocity grid
 // under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
 __host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
+// source window in FP32 (read by two passes), forward / backward windows in binary16
 __host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
-  return sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2 + kDyeW3 * kDyeW3) +
+  return sizeof(float4) * (kDyeW3 * kDyeW3) + sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2) +
          sizeof(float2) * (kDyeW2 * kDyeW2 + kDyeTile * kDyeTile + dye_vel_edge(n, m) * dye_vel_edge(n, m));
 }
 
@@ -222,25 +226,28 @@ __device__ __forceinline__ Rgb rgb_of(uint2 u) {
 // binary16 texel (r, g, b, alpha 1) of FP32 channels, as a texture store rounds them
 __device__ __forceinline__ uint2 pack_rgb(const Rgb& c) { return pack_texel(c.r, c.g, c.b, 1.f); }
 
-// on-chip window of binary16 texels with an exact global fallback (coordinates are wrapped indices)
+__device__ __forceinline__ Rgb rgb_of(float4 v) { return {v.x, v.y, v.z}; }
+
+// on-chip window of source texels (FP32 r, g, b) with an exact global fallback
+// (coordinates are wrapped indices)
 struct SmemTex {
-  const uint2* sm;
+  const float4* sm;
   int ox, oy, w, m;
   const uint2* g;
-  __device__ __forceinline__ uint2 operator()(int x, int y) const {
+  __device__ __forceinline__ Rgb operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return sm[ry * w + rx];
-    return __ldg(g + (size_t)y * m + x);
+    if (rx < w && ry < w) return rgb_of(sm[ry * w + rx]);
+    return rgb_of(__ldg(g + (size_t)y * m + x));
   }
   // the 2x2 footprint in one window test (slots rx, rx+1 hold texels x0, x1 = x0+1 wrapped)
-  __device__ __forceinline__ bool quad(const Footprint& f, uint2 (&c)[4]) const {
+  __device__ __forceinline__ bool quad(const Footprint& f, Rgb (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
     if (rx + 1 < w && ry + 1 < w) {
-      const uint2* p = sm + ry * w + rx;
-      c[0] = p[0];
-      c[1] = p[1];
-      c[2] = p[w];
-      c[3] = p[w + 1];
+      const float4* p = sm + ry * w + rx;
+      c[0] = rgb_of(p[0]);
+      c[1] = rgb_of(p[1]);
+      c[2] = rgb_of(p[w]);
+      c[3] = rgb_of(p[w + 1]);
       return true;
     }
     return false;
@@ -294,14 +301,14 @@ __device__ __forceinline__ float2 sample_vel(const WinVel& w, float px, float py
 // (the same per-channel arithmetic as bilerp)
 template <class TF>
 __device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) {
-  uint2 q[4];
+  Rgb q[4];
   if (!tf.quad(f, q)) {
     q[0] = tf(f.x0, f.y0);
     q[1] = tf(f.x1, f.y0);
     q[2] = tf(f.x0, f.y1);
     q[3] = tf(f.x1, f.y1);
   }
-  const Rgb c00 = rgb_of(q[0]), c10 = rgb_of(q[1]), c01 = rgb_of(q[2]), c11 = rgb_of(q[3]);
+  const Rgb c00 = q[0], c10 = q[1], c01 = q[2], c11 = q[3];
   if (lo) {
     lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
     lo->g = fminf(fminf(c00.g, c10.g), fminf(c01.g, c11.g));
@@ -320,19 +327,19 @@ struct DerivedTex {
   const uint2* sm;
   int ox, oy, w, m;
   const EVAL& eval;
-  __device__ __forceinline__ uint2 operator()(int x, int y) const {
+  __device__ __forceinline__ Rgb operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return sm[ry * w + rx];
-    return eval(x, y);
+    if (rx < w && ry < w) return rgb_of(sm[ry * w + rx]);
+    return rgb_of(eval(x, y));
   }
-  __device__ __forceinline__ bool quad(const Footprint& f, uint2 (&c)[4]) const {
+  __device__ __forceinline__ bool quad(const Footprint& f, Rgb (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
     if (rx + 1 < w && ry + 1 < w) {
       const uint2* p = sm + ry * w + rx;
-      c[0] = p[0];
-      c[1] = p[1];
-      c[2] = p[w];
-      c[3] = p[w + 1];
+      c[0] = rgb_of(p[0]);
+      c[1] = rgb_of(p[1]);
+      c[2] = rgb_of(p[w]);
+      c[3] = rgb_of(p[w + 1]);
       return true;
     }
     return false;
@@ -377,11 +384,11 @@ __global__ void __launch_bounds__(kDyeThreads)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
                 const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
                 const DevSplats* __restrict__ S, int n, int m) {
-  extern __shared__ uint2 dsm2[];
-  uint2* s_back = dsm2;
+  extern __shared__ float4 dsm4[];
+  float4* s_src = dsm4;
+  uint2* s_back = reinterpret_cast<uint2*>(s_src + kDyeW3 * kDyeW3);
   uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
-  uint2* s_src = s_fwd + kDyeW2 * kDyeW2;
-  float2* s_v1 = reinterpret_cast<float2*>(s_src + kDyeW3 * kDyeW3);   // velocity at forward-region texels
+  float2* s_v1 = reinterpret_cast<float2*>(s_fwd + kDyeW2 * kDyeW2);   // velocity at forward-region texels
   float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // forward trace positions of the tile
   float2* s_vel = s_sp + kDyeTile * kDyeTile;
   const int vw = dye_vel_edge(n, m);
@@ -390,17 +397,18 @@ __global__ void __launch_bounds__(kDyeThreads)
   const float h = __fdiv_rn(dtbuf[0], kTwoPiF);
 
   // origins (wrapped) of the on-chip windows
-  const int sx0 = (tx0 - 3 * kDyeHalo) & (m - 1), sy0 = (ty0 - 3 * kDyeHalo) & (m - 1);
-  const int fx0 = (tx0 - 2 * kDyeHalo) & (m - 1), fy0 = (ty0 - 2 * kDyeHalo) & (m - 1);
-  const int bx0 = (tx0 - kDyeHalo) & (m - 1), by0 = (ty0 - kDyeHalo) & (m - 1);
-  const int vx0 = (int)floorf(((float)(tx0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
-  const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeHalo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  const int sx0 = (tx0 - 3 * kDyeLo) & (m - 1), sy0 = (ty0 - 3 * kDyeLo) & (m - 1);
+  const int fx0 = (tx0 - 2 * kDyeLo) & (m - 1), fy0 = (ty0 - 2 * kDyeLo) & (m - 1);
+  const int bx0 = (tx0 - kDyeLo) & (m - 1), by0 = (ty0 - kDyeLo) & (m - 1);
+  const int vx0 = (int)floorf(((float)(tx0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
 
 #pragma unroll 4
   for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
     const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
-    s_src[i] = __ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
+    const Rgb c = rgb_of(__ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1))));
+    s_src[i] = make_float4(c.r, c.g, c.b, 0.f);
   }
 #pragma unroll 4
   for (int i = tid; i < vw * vw; i += kDyeThreads) {
@@ -424,7 +432,7 @@ __global__ void __launch_bounds__(kDyeThreads)
     const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
     const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
     const float2 sp = trace_from(WinVel{V}, p.x, p.y, s_v1[i], h, n);
-    const int tx = rx - 2 * kDyeHalo, ty = ry - 2 * kDyeHalo;
+    const int tx = rx - 2 * kDyeLo, ty = ry - 2 * kDyeLo;
     if ((unsigned)tx < (unsigned)kDyeTile && (unsigned)ty < (unsigned)kDyeTile) s_sp[ty * kDyeTile + tx] = sp;
     s_fwd[i] = pack_rgb(bilerp_rgb(T, footprint(sp.x, sp.y, m)));
   }
@@ -432,10 +440,10 @@ __global__ void __launch_bounds__(kDyeThreads)
 
   const FwdEval fe{V, T, h, n, m};
   const FwdFetch ff{s_fwd, fx0, fy0, kDyeW2, m, fe};
-  // backward pass over the backward region (nested in the forward region by kDyeHalo)
+  // backward pass over the backward region (nested in the forward region by kDyeLo / kDyeHi)
   for (int i = tid; i < kDyeW1 * kDyeW1; i += kDyeThreads) {
     const int ry = i / kDyeW1, rx = i - ry * kDyeW1;
-    const int fi = (ry + kDyeHalo) * kDyeW2 + rx + kDyeHalo;
+    const int fi = (ry + kDyeLo) * kDyeW2 + rx + kDyeLo;
     const float2 p = texel_pos((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1), m);
     const float2 sb = trace_from(WinVel{V}, p.x, p.y, s_v1[fi], -h, n);
     s_back[i] = pack_rgb(bilerp_rgb(ff, footprint(sb.x, sb.y, m)));
