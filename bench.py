@@ -108,16 +108,49 @@ def committed_traffic(kernel):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    NVML is polled every 2 ms on a thread (the timed region can be tens of
+    milliseconds, shorter than nvidia-smi's own sampling start-up); only samples
+    taken between mark_start() and mark_end() count.  nvidia-smi -lms 100 is the
+    fallback when NVML is unavailable.  Read-only: no setting of the GPU changes.
+    """
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
+        self.samples = []            # (time, sm_mhz, reasons bitmask)
+        self.smax = None
+        self.t0 = self.t1 = None
+        self.stop_flag = threading.Event()
+        self.nvml = None
         self.proc = None
         self.lines = []
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
     def start(self):
+        try:
+            self.nvml, self.h = self._nvml_handle()
+            self.smax = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -127,23 +160,56 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml, self.h
+        while not self.stop_flag.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+
+    def _in_window(self, t):
+        return (self.t0 is None or t >= self.t0) and (self.t1 is None or t <= self.t1)
 
     def stop(self):
+        self.stop_flag.set()
+        sm, reasons = [], set()
+        if self.nvml is not None:
+            self.thread.join(timeout=2)
+            for t, mhz, rs in self.samples:
+                if not self._in_window(t):
+                    continue
+                sm.append(mhz)
+                for nm, bit in self.REASONS:
+                    if rs & bit:
+                        reasons.add(nm)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 2 ms polling"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, smax, reasons = [], None, set()
+        smax = None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 9 or not self._in_window(t):
                 continue
             try:
                 sm.append(float(parts[1]))
@@ -154,7 +220,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi -lms 100"}
 
 
 # ------------------------------------------------------------------ distributed plumbing
@@ -270,13 +336,16 @@ def run_ours(args):
     # ---- device-timed region
     clocks = ClockSampler(dev)
     clocks.start()
+    time.sleep(0.05)                      # the poller is running before the timed region
     barrier(world)
     torch.cuda.synchronize(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
     ev0.record(stream)
     solver.step(args.steps, dye=True, reduce=True, graph=True, relatch=True)
     ev1.record(stream)
     ev1.synchronize()
+    clocks.mark_end()
     torch.cuda.synchronize(dev)
     barrier(world)
     clk = clocks.stop()
