@@ -52,11 +52,24 @@ __device__ __forceinline__ float hashf(uint32_t a, uint32_t b) {
   return __uint2float_rn(hash1(a ^ hash1(b))) * 2.3283064365386963e-10f;
 }
 
-// k^(2p) as (k2)^p for integer p >= 0
+// k^(2p) as (k2)^p for integer p >= 0: ((k2 k2) k2) ... left to right, unrolled up
+// to p = 8 (the viscosity orders used) with a loop beyond
 __device__ __forceinline__ float powi(float k2, int p) {
   float r = 1.f;
-  for (int i = 0; i < p; ++i) r *= k2;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    if (i < p) r *= k2;
+  for (int i = 8; i < p; ++i) r *= k2;
   return r;
+}
+
+// k2 outside [lo2, hi2] has forcing envelope exp(-((|k| - K)/W)^2) below 1e-4, the
+// reference's cut: |(|k| - K)/W| > 3.05 > sqrt(ln 1e4) = 3.035 (a conservative
+// pre-test; cells inside run the exact test)
+__device__ __forceinline__ float2 forcing_k2_bounds(const DevParams& P) {
+  const float lo = fmaxf(P.force_k - 3.05f * fabsf(P.force_width), 0.f);
+  const float hi = P.force_k + 3.05f * fabsf(P.force_width);
+  return make_float2(lo * lo, hi * hi);
 }
 
 // White-in-time stochastic forcing of one spectral cell (solver.wgsl:77-92).

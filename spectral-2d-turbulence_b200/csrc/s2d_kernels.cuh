@@ -287,31 +287,48 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
   if constexpr (TU::PREFETCH) mbar_wait_bounded(bar, parity, a.err, 1);
 
   // RK3 stage update, one cell per iteration (kept rolled: the forcing and
-  // integrating-factor code appears once in the kernel, not 16 times)
+  // integrating-factor code appears once in the kernel, not 16 times); the state
+  // (and pointer-force) values of the next cell are loaded one iteration ahead so
+  // their latency overlaps this cell's arithmetic
   {
     const DevParams& P = *a.params;
     float dt = 0.f;
     if constexpr (MODE >= 0) dt = __ldg(a.dt);
+    const float2 fb = forcing_k2_bounds(P);
+    const float2 zero2 = make_float2(0.f, 0.f);
+    auto ld_wc = [&](int c) { return TU::PREFETCH ? s_wcur[c] : a.wcur[rbase + c]; };
+    auto ld_w0 = [&](int c) { return TU::PREFETCH ? s_w0[c] : a.w0[rbase + c]; };
+    auto ld_fp = [&](int c) { return TU::PREFETCH ? s_fptr[c] : __ldg(a.fptr + rbase + c); };
+    float2 wc_next = ld_wc(t), w0_next = zero2, fp_next = zero2;
+    if constexpr (MODE >= 1) w0_next = ld_w0(t);
+    if constexpr (PTR && MODE >= 0) fp_next = ld_fp(t);
 #pragma unroll 1
     for (int m = 0; m < V; ++m) {
       const int c = t + T * m;
       const size_t o = rbase + c;
+      const float2 wc = wc_next;
+      const float2 w0v = w0_next, fpv = fp_next;
+      if (m + 1 < V) {
+        wc_next = ld_wc(c + T);
+        if constexpr (MODE >= 1) w0_next = ld_w0(c + T);
+        if constexpr (PTR && MODE >= 0) fp_next = ld_fp(c + T);
+      }
       float2 w;
       if constexpr (MODE < 0) {
-        w = TU::PREFETCH ? s_wcur[c] : a.wcur[o];
+        w = wc;
       } else {
         const float kx = wn<N>(c);
         const float k2 = kx * kx + ky * ky;
-        const float2 wc = TU::PREFETCH ? s_wcur[c] : a.wcur[o];
-        const float2 w0 = MODE == 0 ? wc : (TU::PREFETCH ? s_w0[c] : a.w0[o]);
+        const float2 w0 = MODE == 0 ? wc : w0v;
         const bool band = row_band && fabsf(kx) < KCUT;
-        const float2 nhat = any_band ? own1[PL::pad(c)] : make_float2(0.f, 0.f);
+        const float2 nhat = any_band ? own1[PL::pad(c)] : zero2;
         float2 rhs = make_float2(-nhat.x, -nhat.y);
         if constexpr (PTR) {
-          if (band) rhs = cadd(rhs, TU::PREFETCH ? s_fptr[c] : __ldg(a.fptr + o));
+          if (band) rhs = cadd(rhs, fpv);
         }
-        if (a.stochastic && band && k2 > 0.f) rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
-        w = k2 == 0.f ? make_float2(0.f, 0.f) : rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
+        if (a.stochastic && band && k2 > 0.f && k2 >= fb.x && k2 <= fb.y)
+          rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
+        w = k2 == 0.f ? zero2 : rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
         a.wout[o] = w;
       }
       own1[PL::pad(c)] = w;
