@@ -96,13 +96,51 @@ __device__ __forceinline__ float2 stochastic_term(const DevParams& P, int n, int
 // exp(x) for |x| ~ 1e-5 rounded to FP32 keeps only ~3 digits of 1 - E, which
 // biases the damping by ~1e-5 per hundred steps; expm1 and the half-angle form
 // cos(t) - 1 = -2 sin^2(t/2) avoid the cancellation.
+//
+// e^x - 1: for |x| < 1/4 the Taylor series to x^7/7! (truncation below
+// |x|^7/8! < 1.5e-9 relative), else expf(x) - 1, which has no cancellation there
+// (|e^x - 1| >= 0.22) and saturates to -1 / overflows to inf like expm1.
+__device__ __forceinline__ float expm1_series(float x) {
+  if (fabsf(x) < 0.25f) {
+    float p = 1.f / 5040.f;
+    p = fmaf(p, x, 1.f / 720.f);
+    p = fmaf(p, x, 1.f / 120.f);
+    p = fmaf(p, x, 1.f / 24.f);
+    p = fmaf(p, x, 1.f / 6.f);
+    p = fmaf(p, x, 0.5f);
+    p = fmaf(p, x, 1.f);
+    return p * x;
+  }
+  return expf(x) - 1.f;
+}
+// sin and cos of a: Taylor series for |a| <= pi/4 (sin to a^9/9!, cos to a^10/10!;
+// truncation below 3e-9 relative), sincosf beyond.
+__device__ __forceinline__ void sincos_series(float a, float* s, float* c) {
+  if (fabsf(a) <= 0.78539816f) {
+    const float a2 = a * a;
+    float ps = 1.f / 362880.f;
+    ps = fmaf(ps, a2, -1.f / 5040.f);
+    ps = fmaf(ps, a2, 1.f / 120.f);
+    ps = fmaf(ps, a2, -1.f / 6.f);
+    ps = fmaf(ps, a2, 1.f);
+    float pc = -1.f / 3628800.f;
+    pc = fmaf(pc, a2, 1.f / 40320.f);
+    pc = fmaf(pc, a2, -1.f / 720.f);
+    pc = fmaf(pc, a2, 1.f / 24.f);
+    pc = fmaf(pc, a2, -0.5f);
+    *s = ps * a;
+    *c = fmaf(pc, a2, 1.f);
+    return;
+  }
+  sincosf(a, s, c);
+}
 __device__ __forceinline__ float2 half_factor_m1(const DevParams& P, float kx, float k2, float dt) {
   const float re = -P.mu - P.nu_h * powi(k2, P.hyper_p);
-  const float d = expm1f(re * (0.5f * dt));
+  const float d = expm1_series(re * (0.5f * dt));
   if (P.beta == 0.f) return make_float2(d, 0.f);
-  const float th = P.beta * kx / k2 * (0.5f * dt);
+  const float th = P.beta * __fdividef(kx, k2) * (0.5f * dt);
   float sh, ch;
-  sincosf(0.5f * th, &sh, &ch);
+  sincos_series(0.5f * th, &sh, &ch);
   const float g = -2.f * sh * sh;         // cos(th) - 1
   const float sn = 2.f * sh * ch;         // sin(th)
   return make_float2(d + g + d * g, (1.f + d) * sn);
@@ -126,9 +164,9 @@ __device__ __forceinline__ float2 rk_update(float2 e, float2 w0, float2 wcur, fl
     return apply_m1(full, adv);
   } else if constexpr (S == 1) {
     const float2 one_e = make_float2(1.f + e.x, e.y);
-    const float den = one_e.x * one_e.x + one_e.y * one_e.y;
+    const float rden = __frcp_rn(one_e.x * one_e.x + one_e.y * one_e.y);
     const float2 q = cmul(e, cconj(one_e));
-    const float2 mhalf = make_float2(-q.x / den, -q.y / den);
+    const float2 mhalf = make_float2(-q.x * rden, -q.y * rden);
     const float2 a = apply_m1(e, w0), b = apply_m1(mhalf, adv);
     return make_float2(0.75f * a.x + 0.25f * b.x, 0.75f * a.y + 0.25f * b.y);
   } else {
