@@ -847,10 +847,9 @@ extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
   const int n = s->n, nb = s->nbins;
   S2D_CUDA(cudaMemsetAsync(s->diag, 0, sizeof(double) * (nb + 2), s->stream));
   S2D_CUDA(cudaMemsetAsync(s->diag_fixed, 0, sizeof(uint32_t) * (nb + 2), s->stream));
-  const unsigned blocks = std::min<unsigned>(cells_grid(n), 148u * 4u);
-  k_diag_spectrum<<<blocks, 256, sizeof(double) * (nb + 2), s->stream>>>(s->state[s->phase], s->diag, n);
-  S2D_LAUNCHED();
-  k_diag_fixed<<<cells_grid(n), 256, 0, s->stream>>>(s->state[s->phase], s->diag_fixed, n);
+  const unsigned items = (unsigned)((size_t)n * n / kDiagCells);
+  const unsigned blocks = std::min<unsigned>((items + 255) / 256, 148u * 4u);
+  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->diag, s->diag_fixed, n);
   S2D_LAUNCHED();
   k_zonal_mean<<<n, 128, 0, s->stream>>>(s->vel, s->zonal, n);
   S2D_LAUNCHED();

@@ -211,60 +211,107 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 }
 
 // ------------------------------------------------------------------ diagnostics
-// FP64 energy, enstrophy and radial spectrum of the state (spectral2d.py:92-104):
-// per-CTA shared histograms in double, one atomicAdd per bin per CTA.
-// out[0..nbins) spectrum, out[nbins] energy, out[nbins+1] enstrophy.
-__global__ void k_diag_spectrum(const float2* __restrict__ w, double* out, int n) {
+// Both spectra in one pass over the state: the FP64 radial spectrum, energy and
+// enstrophy (spectral2d.py:92-104) and the reference's u32 fixed-point bins,
+// truncating, in the dealias band (spectrum.wgsl:19-39).  A thread takes 8
+// consecutive cells of a row, whose |k| bins
+// change slowly along kx, and adds each run of equal bins once (shared-memory bins
+// per CTA, one global atomic per bin per CTA); totals are warp-reduced.  The u32
+// sums wrap mod 2^32 in any order, so the fixed-point result equals the per-cell
+// atomics bit for bit.
+constexpr int kDiagCells = 8;
+__host__ __device__ constexpr size_t diag_all_smem(int n) {
+  return (sizeof(double) + sizeof(uint32_t)) * (size_t)(n / 2 + 3);
+}
+__global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, double* out, uint32_t* bins, int n) {
   extern __shared__ double hist[];
   const int nb = n / 2 + 1;
-  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) hist[i] = 0.0;
+  uint32_t* fhist = reinterpret_cast<uint32_t*>(hist + nb + 2);
+  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) {
+    hist[i] = 0.0;
+    fhist[i] = 0u;
+  }
   __syncthreads();
   const double n4 = (double)n * n * (double)n * n;
+  const float n2f = (float)n * (float)n;
+  const float kcut = (float)(n / 3.0);
+  const int per_row = n / kDiagCells;
   double ene = 0.0, ens = 0.0;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
-    const int kx = (idx & (n - 1)) < n / 2 ? (idx & (n - 1)) : (idx & (n - 1)) - n;
-    const int row = idx / n;
+  uint32_t fe = 0u, fz = 0u;
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n * per_row; it += gridDim.x * blockDim.x) {
+    const int row = it / per_row, c0 = (it - row * per_row) * kDiagCells;
     const int ky = row < n / 2 ? row : row - n;
-    const double k2 = (double)kx * kx + (double)ky * ky;
-    const float2 a = w[idx];
-    const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) / n4;
-    ens += z;
-    if (k2 > 0.0) {
-      const double e = z / k2;
-      ene += e;
-      int b = (int)floor(sqrt(k2) + 0.5);
-      b = b < nb - 1 ? b : nb - 1;
-      atomicAdd(&hist[b], e);
+    const float kyf = (float)ky;
+    const float4* p = reinterpret_cast<const float4*>(w + (size_t)row * n + c0);
+    float2 v[kDiagCells];
+#pragma unroll
+    for (int q = 0; q < kDiagCells / 2; ++q) {
+      const float4 t = p[q];
+      v[2 * q] = make_float2(t.x, t.y);
+      v[2 * q + 1] = make_float2(t.z, t.w);
     }
+    int cur_b = -1, cur_fb = -1;
+    double cur_e = 0.0;
+    uint32_t cur_f = 0u;
+#pragma unroll
+    for (int j = 0; j < kDiagCells; ++j) {
+      const int col = c0 + j;
+      const int kx = col < n / 2 ? col : col - n;
+      const float2 a = v[j];
+      // FP64
+      const double k2 = (double)kx * kx + (double)ky * ky;
+      const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) / n4;
+      ens += z;
+      if (k2 > 0.0) {
+        const double e = z / k2;
+        ene += e;
+        int b = (int)floor(sqrt(k2) + 0.5);
+        b = b < nb - 1 ? b : nb - 1;
+        if (b != cur_b) {
+          if (cur_b >= 0) atomicAdd(&hist[cur_b], cur_e);
+          cur_b = b;
+          cur_e = 0.0;
+        }
+        cur_e += e;
+      }
+      // u32 fixed point
+      const float kxf = (float)kx;
+      const float k2f = kxf * kxf + kyf * kyf;
+      if (k2f != 0.f && fabsf(kxf) < kcut && fabsf(kyf) < kcut) {
+        const float ensf = 0.5f * (a.x * a.x + a.y * a.y) / (n2f * n2f);
+        const float enef = ensf / k2f;
+        const int fb = (int)min((uint32_t)(sqrtf(k2f) + 0.5f), (uint32_t)(nb - 1));
+        if (fb != cur_fb) {
+          if (cur_fb >= 0) atomicAdd(&fhist[cur_fb], cur_f);
+          cur_fb = fb;
+          cur_f = 0u;
+        }
+        cur_f += (uint32_t)(enef * 1e8f);
+        fe += (uint32_t)(enef * 1e6f);
+        fz += (uint32_t)(ensf * 1e6f);
+      }
+    }
+    if (cur_b >= 0) atomicAdd(&hist[cur_b], cur_e);
+    if (cur_fb >= 0) atomicAdd(&fhist[cur_fb], cur_f);
   }
   ene = warp_sum(ene);
   ens = warp_sum(ens);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    fe += __shfl_xor_sync(0xffffffffu, fe, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&hist[nb], ene);
     atomicAdd(&hist[nb + 1], ens);
+    atomicAdd(&fhist[nb], fe);
+    atomicAdd(&fhist[nb + 1], fz);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x)
+  for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) {
     if (hist[i] != 0.0) atomicAdd(&out[i], hist[i]);
-}
-
-// fixed-point accumulation exactly as spectrum.wgsl:19-39 (u32, truncating)
-__global__ void k_diag_fixed(const float2* __restrict__ w, uint32_t* bins, int n) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n * n) return;
-  const int nb = n / 2 + 1;
-  const float kcut = (float)(n / 3.0);
-  const float kx = wn_rt(idx & (n - 1), n), ky = wn_rt(idx / n, n);
-  const float k2 = kx * kx + ky * ky;
-  if (k2 == 0.f || !(fabsf(kx) < kcut && fabsf(ky) < kcut)) return;
-  const float2 a = w[idx];
-  const float n2 = (float)n * (float)n;
-  const float ens = 0.5f * (a.x * a.x + a.y * a.y) / (n2 * n2);
-  const float ene = ens / k2;
-  const uint32_t b = min((uint32_t)(sqrtf(k2) + 0.5f), (uint32_t)(nb - 1));
-  atomicAdd(&bins[b], (uint32_t)(ene * 1e8f));
-  atomicAdd(&bins[nb], (uint32_t)(ene * 1e6f));
-  atomicAdd(&bins[nb + 1], (uint32_t)(ens * 1e6f));
+    if (fhist[i] != 0u) atomicAdd(&bins[i], fhist[i]);
+  }
 }
 
 // zonal mean of u per row (spectrum.wgsl:41-68), accumulated in FP64
