@@ -18,7 +18,8 @@ weak scaling).  ``e2e`` is the same metric through the public Solver API with
 per-step host->device parameter/splat uploads and a device->host diagnostics
 read inside the timed region.  ``roofline`` covers the dominant kernel,
 ``cpu_baseline`` the FP64 NumPy restatement of reference/spectral2d.py on the
-host, ``ensemble`` the batched 256 x 256^2 ensemble.
+host, ``ensemble`` the batched 256 x 256^2 ensemble, ``ensemble_mixed`` the mixed batch
+128 x 128^2 + 256 x 256^2 + 32 x 512^2.
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port of
 reference/spectral2d.py, NumPy FP64) on the same workload with every host core
@@ -422,9 +423,10 @@ def run_ours(args):
         tc = run_tc_leg(pkg, torch, world, rank, dev, args, value, world * args.steps / (ms_rk3 / 1e3))
 
     # ---- batched ensemble: 256 instances of 256^2 (sharded across ranks)
-    ens = None
+    ens = ens_mixed = None
     if not args.no_ensemble:
         ens = run_ensemble(pkg, torch, world, rank, dev, args)
+        ens_mixed = run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_MIXED, seed=4321)
 
     cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
@@ -450,6 +452,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "tc_vs_fp32": tc,
             "ensemble": ens,
+            "ensemble_mixed": ens_mixed,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -532,14 +535,23 @@ def working_set(n, m):
     return 8 * n * n * 7 + 8 * m * m * 3
 
 
-def run_ensemble(pkg, torch, world, rank, dev, args):
+ENSEMBLE_256 = ((256, 256),)
+# the mixed batch of the reference's ensemble configuration: 128 x 128^2, 256 x 256^2, 32 x 512^2
+ENSEMBLE_MIXED = ((128, 128), (256, 256), (512, 32))
+
+
+def run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_256, seed=1234):
+    """Graph-replayed RK3 steps of a batch of independent instances (sizes `groups` =
+    (n, count) pairs), per-instance nu ~ U[1e-4, 1e-3], beta ~ U[0, 20], drag ~ U[0, 2e-2],
+    band-limited initial fields; instances sharded round-robin across ranks."""
     import numpy as np
-    rng = np.random.default_rng(1234)
-    count_total = 256
+    rng = np.random.default_rng(seed)
     inst = []
-    for i in range(count_total):
-        inst.append({"n": 256, "beta": float(rng.uniform(0, 20)), "drag": float(rng.uniform(0, 2e-2)),
-                     "nuH": float(rng.uniform(1e-4, 1e-3)), "hyperP": 1, "dt": 2e-3, "seed": i})
+    for n, count in groups:
+        for _ in range(count):
+            inst.append({"n": n, "beta": float(rng.uniform(0, 20)), "drag": float(rng.uniform(0, 2e-2)),
+                         "nuH": float(rng.uniform(1e-4, 1e-3)), "hyperP": 1, "dt": 2e-3, "seed": len(inst)})
+    count_total = len(inst)
     mine = inst[rank::world]
     e = pkg.Ensemble(mine, device=dev)
     e.seedBand(4.0, 12.0, rms=1.0)
@@ -561,9 +573,10 @@ def run_ensemble(pkg, torch, world, rank, dev, args):
     e.destroy()
     hbm, _, _ = load_peaks()
     ens_steps_per_s = steps / (ms / 1e3)
-    bytes_step = step_algorithmic_bytes(256) * count_total
+    bytes_step = sum(step_algorithmic_bytes(n) * c for n, c in groups)
     gbs = bytes_step * ens_steps_per_s / 1e9
-    return {"instances": count_total, "n": 256, "ensemble_steps_per_s": ens_steps_per_s,
+    return {"instances": count_total, "sizes": {str(n): c for n, c in groups},
+            "n": groups[0][0] if len(groups) == 1 else None, "ensemble_steps_per_s": ens_steps_per_s,
             "instance_steps_per_s": ens_steps_per_s * count_total, "ms_per_ensemble_step": ms / steps,
             "achieved_gbs": gbs, "hbm_peak_gbs": hbm, "frac_of_hbm": gbs / hbm, "finite": ok,
             "note": "232 N^2 algorithmic bytes per instance-step; per-instance nu, beta, drag; graph-replayed"}

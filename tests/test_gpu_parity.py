@@ -94,6 +94,40 @@ def test_fused_step_vs_oracle(pkg, case):
         s.destroy()
 
 
+BIG_CASES = [
+    # n, beta, mu, p, dt, amplitude -- the beta-plane configuration's coefficients at 4096^2
+    # (hyperviscosity as the damping rate 1 at the cutoff)
+    (2048, 0.0, 1e-2, 4, 1e-3, 8.0),
+    (4096, 10.0, 5e-3, 4, 5e-4, 8.0),
+]
+
+
+@pytest.mark.parametrize("case", BIG_CASES, ids=[f"n{c[0]}" for c in BIG_CASES])
+def test_fused_step_vs_oracle_large_grids(pkg, case):
+    """One fused step at 2048^2 and 4096^2 (the 4096 tile shape: 2 columns per CTA)
+    vs the FP64 oracle, rel L2 <= 1e-5."""
+    n, beta, mu, p, dt, amp = case
+    nu_h = 1.0 / (n / 3.0) ** (2 * p)
+    ref = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
+    ref.set_vorticity(random_field(n, k0=n / 16, seed=n + 1, amplitude=amp))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(beta=beta, drag=mu, viscosity=rate_for(nu_h, n, p), hyperP=p))
+        load_state(s, w_in)
+        set_fixed_dt(s, dt)
+        s.setSplats([])
+        s.encodeStep()
+        got = current_state(s)
+    finally:
+        s.destroy()
+    ref.step(dt=dt)
+    err = rel_l2(got, ref.w)
+    print(f"n={n} one step rel L2 {err:.3e}")
+    assert err <= 1e-5, f"one step rel L2 {err:.3e}"
+
+
 def test_out_of_band_overflow_is_contained(pkg):
     """E(-dt/2) = exp(+205) beyond the dealias band overflows in FP32; the reference
     shader forms inf * 0 = NaN there (solver.wgsl:121).  Zero modes must stay zero and
