@@ -153,6 +153,23 @@ int s2d_paint_dye(s2d_solver* s, int pattern);                           /* solv
  * counterpart (the reference seeds with fillSpectrum or a physical field). */
 int s2d_seed_band(s2d_solver* s, float kmin, float kmax, float rms, uint32_t seed);
 
+/* Scenario initial fields (scenarios.js:3-163, SCENARIOS).  `param` is
+ * cfg.mergerSep for MERGER (scenarios.js:137) and cfg.polygonN for POLYGON
+ * (scenarios.js:158, rounded, 1..S2D_SCENARIO_MAX_BLOBS), ignored otherwise.
+ * The field is evaluated on the device in FP64 and rounded to FP32, as the
+ * reference's Float32Array holds it. */
+#define S2D_SCENARIO_SHEAR_LAYER 0
+#define S2D_SCENARIO_TAYLOR_GREEN 1
+#define S2D_SCENARIO_DIPOLE 2
+#define S2D_SCENARIO_MERGER 3
+#define S2D_SCENARIO_POLYGON 4
+#define S2D_SCENARIO_MAX_BLOBS 256
+/* SCENARIOS[kind].build(n, cfg) (scenarios.js) into host memory, n*n floats row-major */
+int s2d_scenario_field(s2d_solver* s, int kind, double param, float* field_out);
+/* reset({field: SCENARIOS[kind].build(n, cfg), dyePattern}) (main.js:281-283 with
+ * solver.js:420-444), the field never leaving the device */
+int s2d_reset_scenario(s2d_solver* s, int kind, double param, int dye_pattern);
+
 /* ---------------------------------------------------------------- step */
 int s2d_encode_prime(s2d_solver* s);                                     /* solver.js:475-486 */
 int s2d_encode_step(s2d_solver* s);                                      /* solver.js:488-521 */

@@ -8,10 +8,12 @@ library and a B200 the calls raise.
 """
 from ._lib import LIB_PATH, S2DError, lib
 from .ensemble import Ensemble
+from .scenarios import SCENARIO_NAMES, SCENARIOS
 from .solver import (MAX_SPLATS, Fft2D, Solver, dealiasMaskTable, digitReverseTable, radixSchedule,
                      supportedGrids, wavenumberTable)
 
 __all__ = [
     "Solver", "Fft2D", "Ensemble", "S2DError", "MAX_SPLATS", "radixSchedule", "supportedGrids",
-    "digitReverseTable", "wavenumberTable", "dealiasMaskTable", "lib", "LIB_PATH",
+    "digitReverseTable", "wavenumberTable", "dealiasMaskTable", "lib", "LIB_PATH", "SCENARIOS",
+    "SCENARIO_NAMES",
 ]

@@ -30,6 +30,12 @@ S2D_FFT_TC_F16 = 1
 S2D_FFT_TC_BF16 = 2
 S2D_DYE_NONE = 0
 S2D_DYE_BANDS = 1
+S2D_SCENARIO_SHEAR_LAYER = 0
+S2D_SCENARIO_TAYLOR_GREEN = 1
+S2D_SCENARIO_DIPOLE = 2
+S2D_SCENARIO_MERGER = 3
+S2D_SCENARIO_POLYGON = 4
+S2D_SCENARIO_MAX_BLOBS = 256
 
 BUFFER_IDS = {
     "state0": 0, "state1": 1, "state2": 2, "packA": 3, "packB": 4, "physZ": 5,
@@ -93,6 +99,8 @@ PROTOTYPES = {
     "s2d_reset": (_i, [_vp, C.POINTER(_f), _d, _d, _u, _i]),
     "s2d_paint_dye": (_i, [_vp, _i]),
     "s2d_seed_band": (_i, [_vp, _f, _f, _f, _u]),
+    "s2d_scenario_field": (_i, [_vp, _i, _d, C.POINTER(_f)]),
+    "s2d_reset_scenario": (_i, [_vp, _i, _d, _i]),
     "s2d_encode_prime": (_i, [_vp]),
     "s2d_encode_step": (_i, [_vp]),
     "s2d_encode_dye": (_i, [_vp]),

@@ -955,25 +955,56 @@ static int check_finite(const float* v, size_t count) {
   return S2D_OK;
 }
 
+// physical field staged (as floats) in the velocity buffer -> packA = (field, 0) -> FFT ->
+// dealias mask into state 0 (solver.js:361-382)
+static float* seed_staging(s2d_solver* s) { return reinterpret_cast<float*>(s->vel); }
+static int seed_from_staging(s2d_solver* s) {
+  const int n = s->n;
+  k_real_to_complex<<<cells_grid(n), 256, 0, s->stream>>>(seed_staging(s), s->packA, n * n);
+  S2D_LAUNCHED();
+  if (int rc = enqueue_fft2(s, s->packA, -1)) return rc;
+  k_seed_mask<<<cells_grid(n), 256, 0, s->stream>>>(s->packA, s->state[0], n);
+  S2D_LAUNCHED();
+  S2D_CUDA(cudaStreamSynchronize(s->stream));   // a host field must outlive its copy
+  s->phase = 0;
+  s->packs_valid = false;
+  s->reduced_valid = false;
+  return zero_other_states(s);
+}
+
 extern "C" int s2d_seed_physical(s2d_solver* s, const float* field) {
   S2D_USE(s);
   if (!field) return fail(S2D_ERR_ARG, "field is null");
   const int n = s->n;
   if (int rc = check_finite(field, (size_t)n * n)) return rc;
   DeviceGuard guard(s->dev);
-  // stage the real field in the velocity buffer, then packA = (field, 0)
-  float* staging = reinterpret_cast<float*>(s->vel);
-  S2D_CUDA(cudaMemcpyAsync(staging, field, sizeof(float) * n * n, cudaMemcpyHostToDevice, s->stream));
-  k_real_to_complex<<<cells_grid(n), 256, 0, s->stream>>>(staging, s->packA, n * n);
+  S2D_CUDA(cudaMemcpyAsync(seed_staging(s), field, sizeof(float) * n * n, cudaMemcpyHostToDevice, s->stream));
+  return seed_from_staging(s);
+}
+
+static int scenario_check(int kind, double param) {
+  if (kind < S2D_SCENARIO_SHEAR_LAYER || kind > S2D_SCENARIO_POLYGON) return fail(S2D_ERR_ARG, "unknown scenario");
+  if (kind == S2D_SCENARIO_MERGER && !std::isfinite(param)) return fail(S2D_ERR_ARG, "mergerSep must be finite");
+  if (kind == S2D_SCENARIO_POLYGON) {
+    const double c = std::floor(param + 0.5);
+    if (!(c >= 1.0 && c <= S2D_SCENARIO_MAX_BLOBS)) return fail(S2D_ERR_ARG, "polygonN out of range");
+  }
+  return S2D_OK;
+}
+
+extern "C" int s2d_scenario_field(s2d_solver* s, int kind, double param, float* field_out) {
+  S2D_USE(s);
+  if (!field_out) return fail(S2D_ERR_ARG, "output is null");
+  if (int rc = scenario_check(kind, param)) return rc;
+  DeviceGuard guard(s->dev);
+  const int n = s->n;
+  // built in the stage-hook rhs buffer; state, packs and velocity are not touched
+  float* tmp = reinterpret_cast<float*>(s->rhs);
+  k_scenario<<<cells_grid(n), 256, 0, s->stream>>>(tmp, n, kind, param);
   S2D_LAUNCHED();
-  if (int rc = enqueue_fft2(s, s->packA, -1)) return rc;
-  k_seed_mask<<<cells_grid(n), 256, 0, s->stream>>>(s->packA, s->state[0], n);
-  S2D_LAUNCHED();
-  S2D_CUDA(cudaStreamSynchronize(s->stream));   // the host field must outlive the copy
-  s->phase = 0;
-  s->packs_valid = false;
-  s->reduced_valid = false;
-  return zero_other_states(s);
+  S2D_CUDA(cudaMemcpyAsync(field_out, tmp, sizeof(float) * n * n, cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
 }
 
 extern "C" int s2d_paint_dye(s2d_solver* s, int pattern) {
@@ -987,6 +1018,9 @@ extern "C" int s2d_paint_dye(s2d_solver* s, int pattern) {
   return S2D_OK;
 }
 
+// the part of reset() after the state is seeded (solver.js:429-443)
+static int reset_after_seed(s2d_solver* s, int dye_pattern);
+
 extern "C" int s2d_reset(s2d_solver* s, const float* field, double k0, double amplitude, uint32_t seed,
                          int dye_pattern) {
   S2D_USE(s);
@@ -997,6 +1031,25 @@ extern "C" int s2d_reset(s2d_solver* s, const float* field, double k0, double am
   s->dye_parity = 0;
   int rc = field ? s2d_seed_physical(s, field) : s2d_seed(s, k0, amplitude, seed);
   if (rc) return rc;
+  return reset_after_seed(s, dye_pattern);
+}
+
+extern "C" int s2d_reset_scenario(s2d_solver* s, int kind, double param, int dye_pattern) {
+  S2D_USE(s);
+  if (dye_pattern != S2D_DYE_NONE && dye_pattern != S2D_DYE_BANDS) return fail(S2D_ERR_ARG, "unknown dye pattern");
+  if (int rc = scenario_check(kind, param)) return rc;
+  DeviceGuard guard(s->dev);
+  s->step_index = 0;
+  s->sim_time = 0.0;
+  s->dye_parity = 0;
+  k_scenario<<<cells_grid(s->n), 256, 0, s->stream>>>(seed_staging(s), s->n, kind, param);
+  S2D_LAUNCHED();
+  if (int rc = seed_from_staging(s)) return rc;
+  return reset_after_seed(s, dye_pattern);
+}
+
+static int reset_after_seed(s2d_solver* s, int dye_pattern) {
+  int rc;
   const size_t dbytes = (size_t)s->m * s->m * sizeof(ushort4);
   for (int i = 0; i < 3; ++i) S2D_CUDA(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream));
   if ((rc = s2d_paint_dye(s, dye_pattern))) return rc;

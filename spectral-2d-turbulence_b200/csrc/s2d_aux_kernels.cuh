@@ -330,6 +330,73 @@ __global__ void k_zonal_mean(const float2* __restrict__ vel, float* zonal, int n
   }
 }
 
+// ------------------------------------------------------------------ scenarios
+// SCENARIOS[kind].build(n, cfg) of scenarios.js, evaluated per cell in FP64 and
+// rounded to FP32 (the reference's Float32Array).  Grid: x = col h, y = row h,
+// h = 2 pi / n (scenarios.js:3-13).
+__device__ __forceinline__ double scen_wrap_delta(double a, double b) {   // scenarios.js:20-28
+  constexpr double kPi = 3.14159265358979323846, k2Pi = 2.0 * kPi;
+  double d = a - b;
+  if (d > kPi) d -= k2Pi;
+  else if (d < -kPi) d += k2Pi;
+  return d;
+}
+// one Gaussian blob of blobs() (scenarios.js:30-44)
+__device__ __forceinline__ double scen_blob(double x, double y, double bx, double by, double a, double amp) {
+  const double dx = scen_wrap_delta(x, bx), dy = scen_wrap_delta(y, by);
+  const double r2 = dx * dx + dy * dy, s2 = a * a;
+  return r2 < 25.0 * s2 ? amp * exp(-r2 / s2) : 0.0;
+}
+__global__ void k_scenario(float* out, int n, int kind, double param) {
+  constexpr double kPi = 3.14159265358979323846, k2Pi = 2.0 * kPi;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  const int row = idx / n, col = idx - row * n;
+  const double h = k2Pi / n;
+  const double x = col * h, y = row * h;
+  double v = 0.0;
+  switch (kind) {
+    case 0: {   // 'shear layer' (scenarios.js:70-79)
+      const double delta = fmax(k2Pi / 30.0, (6.0 * k2Pi) / n);
+      const double eps = 0.05;
+      const bool lower = y <= kPi;
+      const double z = lower ? (y - kPi / 2.0) / delta : (1.5 * kPi - y) / delta;
+      const double c = cosh(z);
+      const double dudy = ((lower ? 1.0 : -1.0) * (1.0 / (c * c))) / delta;
+      v = eps * cos(x) - dudy;
+      break;
+    }
+    case 1:     // 'taylor-green' (scenarios.js:94-97)
+      v = 6.0 * cos(2.0 * x) * cos(2.0 * y);
+      break;
+    case 2: {   // dipole (scenarios.js:112-122)
+      const double gamma = 12.0, a = 0.3, d = 0.9;
+      const double amp = gamma / (kPi * a * a), cx = kPi * 0.6;
+      v = scen_blob(x, y, cx, kPi - d / 2.0, a, amp);
+      v += scen_blob(x, y, cx, kPi + d / 2.0, a, -amp);
+      break;
+    }
+    case 3: {   // merger (scenarios.js:136-143), d = cfg.mergerSep
+      const double a = 0.22, d = param;
+      v = scen_blob(x, y, kPi - d / 2.0, kPi, a, 30.0);
+      v += scen_blob(x, y, kPi + d / 2.0, kPi, a, 30.0);
+      break;
+    }
+    default: {  // polygon: ring(n, round(cfg.polygonN), 1.25, 0.19, 34, 0.02) (scenarios.js:46-56,157-159)
+      const int count = (int)floor(param + 0.5);
+      const double radius = 1.25, a = 0.19, amp = 34.0, jitter = 0.02;
+      const int mode = max(2, count / 2);
+      for (int j = 0; j < count; ++j) {
+        const double th = (k2Pi * j) / count;
+        const double r = radius * (1.0 + jitter * cos((k2Pi * mode * j) / count));
+        v += scen_blob(x, y, kPi + r * cos(th), kPi + r * sin(th), a, amp);
+      }
+      break;
+    }
+  }
+  out[idx] = (float)v;
+}
+
 // ------------------------------------------------------------------ dye
 // JS toHalf (solver.js:20-41): f32 -> binary16 by mantissa truncation
 __device__ __forceinline__ uint16_t to_half_trunc(float value) {

@@ -251,6 +251,17 @@ class Solver:
             L.call("s2d_reset", self._use(), None, float(opts.get("k0", 14)), float(opts.get("amplitude", 6)),
                    int(opts.get("seed", 1)) & 0xFFFFFFFF, pattern)
 
+    def scenarioField(self, name: str, cfg: dict | None = None):
+        """SCENARIOS[name].build(n, cfg) (scenarios.js) evaluated on the GPU: (n, n) float32."""
+        from . import scenarios
+        return scenarios.build(self, name, cfg)
+
+    def resetScenario(self, name: str, cfg: dict | None = None, dyePattern: str = "bands"):
+        """reset({field: SCENARIOS[name].build(n, cfg), dyePattern}) (main.js:281-283), the
+        field built and seeded on the device."""
+        from . import scenarios
+        scenarios.reset(self, name, cfg, dyePattern)
+
     def paintDye(self, pattern: str):
         """solver.js:446-473."""
         if pattern not in _PATTERNS:
