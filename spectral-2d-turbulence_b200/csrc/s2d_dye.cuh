@@ -210,11 +210,21 @@ constexpr int kDyeW3 = kDyeTile + 3 * (kDyeLo + kDyeHi);   // source region edge
 // velocity cells needed by traces from the forward-pass region, for an n x n velocity grid
 // under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
 __host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
-// source window in FP32 (read by two passes), forward / backward windows in binary16
+// binary16 source / forward / backward windows; FP32 centre velocities and forward trace
+// positions of the forward region; the velocity window
 __host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
-  return sizeof(float4) * (kDyeW3 * kDyeW3) + sizeof(uint2) * (kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2) +
-         sizeof(float2) * (kDyeW2 * kDyeW2 + kDyeTile * kDyeTile + dye_vel_edge(n, m) * dye_vel_edge(n, m));
+  return sizeof(uint2) * (kDyeW3 * kDyeW3 + kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2) +
+         sizeof(float2) * (2 * kDyeW2 * kDyeW2 + dye_vel_edge(n, m) * dye_vel_edge(n, m));
 }
+
+// 8-byte asynchronous global -> shared copy (no register staging) and its wait
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 struct Rgb {
   float r, g, b;
@@ -226,12 +236,10 @@ __device__ __forceinline__ Rgb rgb_of(uint2 u) {
 // binary16 texel (r, g, b, alpha 1) of FP32 channels, as a texture store rounds them
 __device__ __forceinline__ uint2 pack_rgb(const Rgb& c) { return pack_texel(c.r, c.g, c.b, 1.f); }
 
-__device__ __forceinline__ Rgb rgb_of(float4 v) { return {v.x, v.y, v.z}; }
-
-// on-chip window of source texels (FP32 r, g, b) with an exact global fallback
-// (coordinates are wrapped indices)
+// on-chip window of binary16 source texels with an exact global fallback (coordinates
+// are wrapped indices)
 struct SmemTex {
-  const float4* sm;
+  const uint2* sm;
   int ox, oy, w, m;
   const uint2* g;
   __device__ __forceinline__ Rgb operator()(int x, int y) const {
@@ -243,7 +251,7 @@ struct SmemTex {
   __device__ __forceinline__ bool quad(const Footprint& f, Rgb (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
     if (rx + 1 < w && ry + 1 < w) {
-      const float4* p = sm + ry * w + rx;
+      const uint2* p = sm + ry * w + rx;
       c[0] = rgb_of(p[0]);
       c[1] = rgb_of(p[1]);
       c[2] = rgb_of(p[w]);
@@ -384,13 +392,13 @@ __global__ void __launch_bounds__(kDyeThreads)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
                 const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
                 const DevSplats* __restrict__ S, int n, int m) {
-  extern __shared__ float4 dsm4[];
-  float4* s_src = dsm4;
-  uint2* s_back = reinterpret_cast<uint2*>(s_src + kDyeW3 * kDyeW3);
+  extern __shared__ uint2 dsm2[];
+  uint2* s_src = dsm2;
+  uint2* s_back = s_src + kDyeW3 * kDyeW3;
   uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
   float2* s_v1 = reinterpret_cast<float2*>(s_fwd + kDyeW2 * kDyeW2);   // velocity at forward-region texels
-  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // forward trace positions of the tile
-  float2* s_vel = s_sp + kDyeTile * kDyeTile;
+  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // their forward trace positions
+  float2* s_vel = s_sp + kDyeW2 * kDyeW2;
   const int vw = dye_vel_edge(n, m);
   const int tx0 = blockIdx.x * kDyeTile, ty0 = blockIdx.y * kDyeTile;
   const int tid = threadIdx.x;
@@ -404,12 +412,13 @@ __global__ void __launch_bounds__(kDyeThreads)
   const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
 
+  // the source window arrives asynchronously while the traces below (velocity only) run
 #pragma unroll 4
   for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
     const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
-    const Rgb c = rgb_of(__ldg(src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1))));
-    s_src[i] = make_float4(c.r, c.g, c.b, 0.f);
+    cp_async8(s_src + i, src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
   }
+  cp_async_commit();
 #pragma unroll 4
   for (int i = tid; i < vw * vw; i += kDyeThreads) {
     const int ry = i / vw, rx = i - ry * vw;
@@ -419,21 +428,21 @@ __global__ void __launch_bounds__(kDyeThreads)
 
   const SmemVel V{s_vel, vxw, vyw, vw, n, vel};
   const SmemTex T{s_src, sx0, sy0, kDyeW3, m, src};
-  // velocity at every forward-region texel centre: shared by the +h and -h traces
+  // velocity at every forward-region texel centre (shared by the +h and -h traces) and
+  // the forward trace from it
   for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
     const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
     const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
-    s_v1[i] = sample_vel_win(V, p.x, p.y);
+    const float2 v1 = sample_vel_win(V, p.x, p.y);
+    s_v1[i] = v1;
+    s_sp[i] = trace_from(WinVel{V}, p.x, p.y, v1, h, n);
   }
+  cp_async_wait_all();
   __syncthreads();
 
-  // forward pass over the forward region; keep the tile's trace positions for the correction
+  // forward pass over the forward region
   for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
-    const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
-    const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
-    const float2 sp = trace_from(WinVel{V}, p.x, p.y, s_v1[i], h, n);
-    const int tx = rx - 2 * kDyeLo, ty = ry - 2 * kDyeLo;
-    if ((unsigned)tx < (unsigned)kDyeTile && (unsigned)ty < (unsigned)kDyeTile) s_sp[ty * kDyeTile + tx] = sp;
+    const float2 sp = s_sp[i];
     s_fwd[i] = pack_rgb(bilerp_rgb(T, footprint(sp.x, sp.y, m)));
   }
   __syncthreads();
@@ -457,7 +466,7 @@ __global__ void __launch_bounds__(kDyeThreads)
     const int ry = i / kDyeTile, rx = i - ry * kDyeTile;
     const int x = tx0 + rx, y = ty0 + ry;
     const float2 p = texel_pos(x, y, m);
-    const float2 sp = s_sp[i];
+    const float2 sp = s_sp[(ry + 2 * kDyeLo) * kDyeW2 + rx + 2 * kDyeLo];
     const Footprint f = footprint(sp.x, sp.y, m);
     Rgb lo, hi;
     const Rgb a = bilerp_rgb(T, f, &lo, &hi);
