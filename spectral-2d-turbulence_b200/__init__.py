@@ -8,6 +8,7 @@ library and a B200 the calls raise.
 """
 from ._lib import LIB_PATH, S2DError, lib
 from .ensemble import Ensemble
+from .pointer import Pointer
 from .scenarios import SCENARIO_NAMES, SCENARIOS
 from .solver import (MAX_SPLATS, Fft2D, Solver, dealiasMaskTable, digitReverseTable, radixSchedule,
                      supportedGrids, wavenumberTable)
@@ -15,5 +16,5 @@ from .solver import (MAX_SPLATS, Fft2D, Solver, dealiasMaskTable, digitReverseTa
 __all__ = [
     "Solver", "Fft2D", "Ensemble", "S2DError", "MAX_SPLATS", "radixSchedule", "supportedGrids",
     "digitReverseTable", "wavenumberTable", "dealiasMaskTable", "lib", "LIB_PATH", "SCENARIOS",
-    "SCENARIO_NAMES",
+    "SCENARIO_NAMES", "Pointer",
 ]
