@@ -170,6 +170,18 @@ int s2d_scenario_field(s2d_solver* s, int kind, double param, float* field_out);
  * solver.js:420-444), the field never leaving the device */
 int s2d_reset_scenario(s2d_solver* s, int kind, double param, int dye_pattern);
 
+/* ---------------------------------------------------------------- headless image */
+/* Renderer.render(encoder, solver, cfg) (render.js:63-87, render.wgsl:81-103) into a
+ * host buffer of height*width RGBA8 pixels, row 0 at the top, instead of a canvas:
+ * mode 0 dye, 1 vorticity, 2 dye over vorticity, 3 speed (render.js:4).  The
+ * vorticity is the current state's (the reference shows the last stage's). */
+#define S2D_RENDER_DYE 0
+#define S2D_RENDER_VORTICITY 1
+#define S2D_RENDER_DYE_OVER_VORTICITY 2
+#define S2D_RENDER_SPEED 3
+int s2d_render(s2d_solver* s, int mode, float exposure, float vort_scale, float dye_gain, int width, int height,
+               void* rgba_out);
+
 /* ---------------------------------------------------------------- step */
 int s2d_encode_prime(s2d_solver* s);                                     /* solver.js:475-486 */
 int s2d_encode_step(s2d_solver* s);                                      /* solver.js:488-521 */

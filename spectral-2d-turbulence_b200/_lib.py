@@ -36,6 +36,7 @@ S2D_SCENARIO_DIPOLE = 2
 S2D_SCENARIO_MERGER = 3
 S2D_SCENARIO_POLYGON = 4
 S2D_SCENARIO_MAX_BLOBS = 256
+RENDER_MODES = ["dye", "vorticity", "dye over vorticity", "speed"]     # render.js:4
 
 BUFFER_IDS = {
     "state0": 0, "state1": 1, "state2": 2, "packA": 3, "packB": 4, "physZ": 5,
@@ -101,6 +102,7 @@ PROTOTYPES = {
     "s2d_seed_band": (_i, [_vp, _f, _f, _f, _u]),
     "s2d_scenario_field": (_i, [_vp, _i, _d, C.POINTER(_f)]),
     "s2d_reset_scenario": (_i, [_vp, _i, _d, _i]),
+    "s2d_render": (_i, [_vp, _i, _f, _f, _f, _i, _i, _vp]),
     "s2d_encode_prime": (_i, [_vp]),
     "s2d_encode_step": (_i, [_vp]),
     "s2d_encode_dye": (_i, [_vp]),

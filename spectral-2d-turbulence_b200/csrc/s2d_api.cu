@@ -17,6 +17,7 @@
 #include "s2d_aux_kernels.cuh"
 #include "s2d_ops.cuh"
 #include "s2d_tc.cuh"
+#include "s2d_render.cuh"
 
 using namespace s2d;
 
@@ -145,6 +146,8 @@ struct s2d_solver {
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
   int* err = nullptr;                 // device error word (bounded waits that gave up)
   char* tctab = nullptr;              // tensor-core DFT32 planes + twiddle matrix (fft 'tc-f16')
+  uchar4* image = nullptr;            // headless render target, grown on demand
+  size_t image_px = 0;
   ushort4* dye[3] = {nullptr, nullptr, nullptr};
   // pinned readback staging (copyDiagnostics)
   double* h_diag = nullptr;
@@ -161,6 +164,7 @@ struct s2d_solver {
   double sim_time = 0.0;
   bool primed = false, packs_valid = false, reduced_valid = false, disposed = false;
   int read_state = 0;  // 0 idle, 1 copied
+  bool latch_pending = false;   // S2D_STEP_RELATCH: the next step's first column kernel latches
   std::map<GraphKey, GraphEntry> graphs;
   // instrumentation: event pairs around launches, by kernel class
   bool profiling = false;
@@ -213,7 +217,7 @@ static void free_solver(s2d_solver* s) {
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
                       s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->dye[0], s->dye[1], s->dye[2]};
+                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->image, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
   void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
@@ -653,6 +657,11 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     {
       ProfScope ps(s, S2D_PROF_PHYS_COLS);
       PhysArgs pa = phys_args(s, st == 2 ? 1 : 0);
+      if (st == 0 && s->latch_pending) {
+        pa.latch = s->dparams;
+        pa.counter = s->step_counter;
+        s->latch_pending = false;
+      }
       enqueue_phys_cols(s, st == 2 ? 2 : 1, pa);
       S2D_LAUNCHED();
     }
@@ -738,9 +747,9 @@ static int sync_step_counter(s2d_solver* s) {
   return S2D_OK;
 }
 
+// stepIndex <- device counter (then counter + 1), done by the next step's first column kernel
 static int enqueue_relatch(s2d_solver* s) {
-  k_latch_step<<<1, 1, 0, s->stream>>>(s->dparams, s->step_counter);
-  S2D_LAUNCHED();
+  s->latch_pending = true;
   return S2D_OK;
 }
 
@@ -1015,6 +1024,34 @@ extern "C" int s2d_paint_dye(s2d_solver* s, int pattern) {
   const int m = s->m;
   k_paint_bands<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, s->stream>>>(s->dye[s->dye_parity], m);
   S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+extern "C" int s2d_render(s2d_solver* s, int mode, float exposure, float vort_scale, float dye_gain, int width,
+                          int height, void* rgba_out) {
+  S2D_USE(s);
+  if (!rgba_out) return fail(S2D_ERR_ARG, "output is null");
+  if (mode < S2D_RENDER_DYE || mode > S2D_RENDER_SPEED) return fail(S2D_ERR_ARG, "unknown render mode");
+  if (width <= 0 || height <= 0 || width > 16384 || height > 16384) return fail(S2D_ERR_ARG, "image size out of range");
+  DeviceGuard guard(s->dev);
+  const size_t px = (size_t)width * height;
+  if (px > s->image_px) {
+    if (s->image) cudaFree(s->image);
+    s->image = nullptr;
+    s->image_px = 0;
+    S2D_CUDA(cudaMalloc(&s->image, px * sizeof(uchar4)));
+    s->image_px = px;
+  }
+  // physical vorticity of the current state in the stage-hook rhs buffer
+  const size_t cbytes = (size_t)s->n * s->n * sizeof(float2);
+  S2D_CUDA(cudaMemcpyAsync(s->rhs, s->state[s->phase], cbytes, cudaMemcpyDeviceToDevice, s->stream));
+  if (int rc = enqueue_fft2(s, s->rhs, +1)) return rc;
+  const dim3 blk(16, 16), grd((width + 15) / 16, (height + 15) / 16);
+  k_render<<<grd, blk, 0, s->stream>>>(s->image, width, height, s->rhs, s->vel, tex(s, s->dye_parity), s->n, s->m,
+                                        mode, exposure, vort_scale, dye_gain);
+  S2D_LAUNCHED();
+  S2D_CUDA(cudaMemcpyAsync(rgba_out, s->image, px * sizeof(uchar4), cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->stream));
   return S2D_OK;
 }
 

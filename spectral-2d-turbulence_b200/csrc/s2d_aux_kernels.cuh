@@ -69,14 +69,6 @@ __global__ void k_pointer_force(float2* force, const DevSplats* __restrict__ S, 
   force[idx] = make_float2(total, 0.f);
 }
 
-// params.step_index = counter++ (one thread): the step index a configure() before
-// this substep would latch (solver.js:316)
-__global__ void k_latch_step(DevParams* params, uint32_t* counter) {
-  const uint32_t k = *counter;
-  params->step_index = k;
-  *counter = k + 1u;
-}
-
 // ------------------------------------------------------------------ CFL reduction (reduce.wgsl:22-63)
 __global__ void k_reduce_speed(const float2* __restrict__ vel, float* partials, int ncells) {
   float m = 0.f;

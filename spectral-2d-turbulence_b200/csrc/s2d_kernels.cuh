@@ -77,7 +77,21 @@ struct PhysArgs {
   const DevParams* params;
   const float2* tw;
   int reduce;           // finalize the CFL dt into dt_out
+  DevParams* latch;     // non-null: latch step_index from *counter (and advance it) first
+  uint32_t* counter;
 };
+
+// the per-substep stepIndex latch (S2D_STEP_RELATCH): params.step_index = counter++,
+// the step index a configure() before this substep would latch (solver.js:316); done by
+// one thread of the first stage's column kernel, since nothing in that kernel reads
+// step_index and its first reader (the row kernel's stochastic forcing) is the next launch
+__device__ __forceinline__ void phys_latch(const PhysArgs& a) {
+  if (a.latch && blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t k = *a.counter;
+    a.latch->step_index = k;
+    *a.counter = k + 1u;
+  }
+}
 
 struct SpecArgs {
   const float2* z;      // product spectrum (ky, x), in-band rows
@@ -203,6 +217,7 @@ template <int N, int MODE>
 __global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_cols(PhysArgs a) {
   using TU = Tune<N>;
   extern __shared__ float2 smem[];
+  phys_latch(a);
   const float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
   if constexpr (MODE != 1) cols_speed_finalize<TU::A_THREADS>(a, speed);
 }

@@ -472,6 +472,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, cons
   const TcMisc m = tc_misc(sm);
   const int tid = threadIdx.x, lane = tid & 31;
   const int x0 = blockIdx.x * kTcCols;
+  phys_latch(a);
   // load: thread (line g, n1 t) takes the pack at ky = t + 32 n2 -- one operand row
   const int g = tid & 7, t = tid >> 3;
   const float2* src = (g < kTcCols ? a.pa : a.pb) + x0 + (g & (kTcCols - 1));

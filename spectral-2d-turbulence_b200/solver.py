@@ -262,6 +262,20 @@ class Solver:
         from . import scenarios
         scenarios.reset(self, name, cfg, dyePattern)
 
+    def render(self, cfg: dict | None = None, width: int | None = None, height: int | None = None):
+        """Renderer.render(encoder, solver, cfg) (render.js:63-87) without a canvas: an
+        (height, width, 4) uint8 RGBA image, row 0 at the top.  cfg keys: mode (render.js:4
+        names), exposure, vortScale, dyeGain; the image defaults to the dye grid's size."""
+        cfg = cfg or {}
+        mode = cfg.get("mode", "dye over vorticity")
+        idx = L.RENDER_MODES.index(mode) if mode in L.RENDER_MODES else 0      # render.js:65
+        w = self.m if width is None else int(width)
+        h = self.m if height is None else int(height)
+        out = np.empty((h, w, 4), np.uint8)
+        L.call("s2d_render", self._use(), idx, float(cfg.get("exposure", 1.3)), float(cfg.get("vortScale", 0.16)),
+               float(cfg.get("dyeGain", 1.0)), w, h, out.ctypes.data_as(C.c_void_p))
+        return out
+
     def paintDye(self, pattern: str):
         """solver.js:446-473."""
         if pattern not in _PATTERNS:

@@ -548,3 +548,29 @@ def test_tc_taylor_green_decay_rate(pkg):
         assert err <= 1e-5
     finally:
         s.destroy()
+
+
+def test_relatch_equals_configure_per_substep(pkg):
+    """S2D_STEP_RELATCH (stepIndex latched by the step's first column kernel) draws the
+    same forcing phases as a configure() before every substep (solver.js:316), directly
+    and through graph replay."""
+    n = 128
+    w = random_field(n, k0=12, seed=9, amplitude=4.0)
+    cfg = config(viscosity=1.0, hyperP=4, forceAmp=0.1, forceK=20.0, forceWidth=2.0, cfl=0.5, dtMax=2e-3)
+    outs = []
+    for mode in ("configure", "relatch", "relatch-graph"):
+        s = pkg.Solver.create(n=n, dyeScale=1)
+        try:
+            s.configure(cfg)
+            s.reset({"field": w, "dyePattern": "none"})
+            for _ in range(4):
+                if mode == "configure":
+                    s.configure(cfg)
+                    s.step(1, dye=False, reduce=True, graph=False)
+                else:
+                    s.step(1, dye=False, reduce=True, graph=(mode == "relatch-graph"), relatch=True)
+            outs.append(current_state(s))
+        finally:
+            s.destroy()
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
