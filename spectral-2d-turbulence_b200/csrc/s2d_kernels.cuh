@@ -343,7 +343,12 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
         }
         if (a.stochastic && band && k2 > 0.f && k2 >= fb.x && k2 <= fb.y)
           rhs = cadd(rhs, stochastic_term(P, N, row, c, kx, ky, k2, dt));
-        w = k2 == 0.f ? zero2 : rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
+        // a cell whose state and right-hand side are all zero stays zero (every stage form
+        // is linear in w0, wcur, rhs): the modes outside the dealias band of a dealiased
+        // state skip the integrating factor
+        const bool quiet = wc.x == 0.f && wc.y == 0.f && w0.x == 0.f && w0.y == 0.f && rhs.x == 0.f && rhs.y == 0.f;
+        if (k2 == 0.f || quiet) w = zero2;
+        else w = rk_update<MODE>(half_factor_m1(P, kx, k2, dt), w0, wc, rhs, dt);
         a.wout[o] = w;
       }
       own1[PL::pad(c)] = w;
