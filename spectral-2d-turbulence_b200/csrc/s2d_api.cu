@@ -146,6 +146,8 @@ struct s2d_solver {
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
   int* err = nullptr;                 // device error word (bounded waits that gave up)
   char* tctab = nullptr;              // tensor-core DFT32 planes + twiddle matrix (fft 'tc-f16')
+  int* row_nz = nullptr;              // per ky row: the last row-kernel pass wrote a nonzero PA/PB row
+  bool packs_flagged = false;         // PA/PB rows flagged zero were left unwritten
   uchar4* image = nullptr;            // headless render target, grown on demand
   size_t image_px = 0;
   ushort4* dye[3] = {nullptr, nullptr, nullptr};
@@ -217,7 +219,7 @@ static void free_solver(s2d_solver* s) {
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
                       s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->image, s->dye[0], s->dye[1], s->dye[2]};
+                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
   void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
@@ -375,6 +377,7 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   const int nparts = std::max(std::max(ops->a_grid, 256), seed_parts_count(n));
   TRY(cudaMalloc(&s->partials, sizeof(float) * nparts), "partials");
   TRY(cudaMalloc(&s->ticket, sizeof(unsigned)), "ticket");
+  TRY(cudaMalloc(&s->row_nz, sizeof(int) * n), "row flags");
   TRY(cudaMalloc(&s->dparams, sizeof(DevParams)), "params");
   TRY(cudaMalloc(&s->dsplats, sizeof(DevSplats)), "splats");
   TRY(cudaMalloc(&s->diag, sizeof(double) * (s->nbins + 2)), "diag");
@@ -591,9 +594,21 @@ static int enqueue_pack_prime(s2d_solver* s) {
   a.params = s->dparams;
   a.tw = s->tw;
   a.err = s->err;
+  a.row_nz = s->row_nz;
   s->ops->spec_rows(-1, false, a, s->stream);
   S2D_LAUNCHED();
+  s->packs_flagged = true;
   s->packs_valid = true;
+  return S2D_OK;
+}
+
+// make the rows the row kernel skipped (flagged all zero) explicit zeros, before anything
+// other than the fused stage kernels reads or writes the packs
+static int materialize_packs(s2d_solver* s) {
+  if (!s->packs_flagged) return S2D_OK;
+  k_zero_flagged_rows<<<cells_grid(s->n), 256, 0, s->stream>>>(s->packA, s->packB, s->row_nz, s->n);
+  S2D_LAUNCHED();
+  s->packs_flagged = false;
   return S2D_OK;
 }
 
@@ -609,6 +624,7 @@ static PhysArgs phys_args(s2d_solver* s, int reduce) {
   a.params = s->dparams;
   a.tw = s->tw;
   a.reduce = reduce;
+  a.row_nz = s->row_nz;
   return a;
 }
 
@@ -679,8 +695,10 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     a.tw = s->tw;
     a.stochastic = s->hp.force_amp > 0.f ? 1 : 0;
     a.err = s->err;
+    a.row_nz = s->row_nz;
     s->ops->spec_rows(st, ptr, a, s->stream);
     S2D_LAUNCHED();
+    s->packs_flagged = true;
   }
   s->reduced_valid = true;
   s->packs_valid = true;
@@ -969,6 +987,7 @@ static int check_finite(const float* v, size_t count) {
 static float* seed_staging(s2d_solver* s) { return reinterpret_cast<float*>(s->vel); }
 static int seed_from_staging(s2d_solver* s) {
   const int n = s->n;
+  if (int rc = materialize_packs(s)) return rc;   // packA is the scratch line here
   k_real_to_complex<<<cells_grid(n), 256, 0, s->stream>>>(seed_staging(s), s->packA, n * n);
   S2D_LAUNCHED();
   if (int rc = enqueue_fft2(s, s->packA, -1)) return rc;
@@ -1123,6 +1142,8 @@ extern "C" int s2d_get_buffer(s2d_solver* s, int id, void* host, size_t bytes) {
   size_t sz = 0;
   if (int rc = buffer_for(s, id, &p, &sz)) return rc;
   DeviceGuard guard(s->dev);
+  if (id == S2D_BUF_PACKA || id == S2D_BUF_PACKB)
+    if (int rc = materialize_packs(s)) return rc;
   if (id == S2D_BUF_DT) {
     if (bytes < sz) return fail(S2D_ERR_ARG, "host buffer too small");
     float tmp[4] = {0, 0, 0, 0};
@@ -1146,6 +1167,8 @@ extern "C" int s2d_set_buffer(s2d_solver* s, int id, const void* host, size_t by
   if (bytes > sz) return fail(S2D_ERR_ARG, "more bytes than the buffer holds");
   if (int rc = check_finite(static_cast<const float*>(host), bytes / sizeof(float))) return rc;
   DeviceGuard guard(s->dev);
+  if (id == S2D_BUF_PACKA || id == S2D_BUF_PACKB)
+    if (int rc = materialize_packs(s)) return rc;
   S2D_CUDA(cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, s->stream));
   S2D_CUDA(cudaStreamSynchronize(s->stream));
   if (id <= S2D_BUF_PACKB) s->packs_valid = false;
@@ -1164,7 +1187,10 @@ extern "C" int s2d_fft2(s2d_solver* s, int id, int inverse) {
     default: return fail(S2D_ERR_UNREGISTERED, "buffer " + std::to_string(id) + " was never registered with the FFT");
   }
   DeviceGuard guard(s->dev);
-  if (id == S2D_BUF_PACKA || id == S2D_BUF_PACKB) s->packs_valid = false;
+  if (id == S2D_BUF_PACKA || id == S2D_BUF_PACKB) {
+    if (int rc = materialize_packs(s)) return rc;
+    s->packs_valid = false;
+  }
   return enqueue_fft2(s, buf, inverse ? +1 : -1);
 }
 
@@ -1172,6 +1198,7 @@ extern "C" int s2d_velocity_pack(s2d_solver* s, int state_index) {
   S2D_USE(s);
   if (state_index < 0 || state_index > 2) return fail(S2D_ERR_ARG, "state index out of range");
   DeviceGuard guard(s->dev);
+  if (int rc = materialize_packs(s)) return rc;
   k_velocity_pack<<<cells_grid(s->n), 256, 0, s->stream>>>(s->state[state_index], s->packA, s->packB, s->n);
   S2D_LAUNCHED();
   s->packs_valid = false;
@@ -1181,6 +1208,7 @@ extern "C" int s2d_velocity_pack(s2d_solver* s, int state_index) {
 extern "C" int s2d_nl_pack(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
+  if (int rc = materialize_packs(s)) return rc;
   k_nl_pack<<<cells_grid(s->n), 256, 0, s->stream>>>(s->packA, s->packB, s->physZ, s->vel, s->n);
   S2D_LAUNCHED();
   s->reduced_valid = false;

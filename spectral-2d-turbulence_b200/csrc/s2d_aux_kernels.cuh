@@ -120,6 +120,16 @@ __global__ void k_seed_mask(const float2* __restrict__ src, float2* dst, int n) 
 }
 
 // real field -> complex (value, 0) (solver.js:363-367)
+// zero the rows of the packs that the row kernel flagged as all zero and left unwritten
+__global__ void k_zero_flagged_rows(float2* pa, float2* pb, const int* __restrict__ row_nz, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  if (row_nz[idx / n] == 0) {
+    pa[idx] = make_float2(0.f, 0.f);
+    pb[idx] = make_float2(0.f, 0.f);
+  }
+}
+
 __global__ void k_real_to_complex(const float* __restrict__ src, float2* dst, int ncells) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ncells) dst[i] = make_float2(src[i], 0.f);

@@ -79,6 +79,7 @@ struct PhysArgs {
   int reduce;           // finalize the CFL dt into dt_out
   DevParams* latch;     // non-null: latch step_index from *counter (and advance it) first
   uint32_t* counter;
+  const int* row_nz;    // non-null: row ky of PA/PB is all zero (and need not be read) where 0
 };
 
 // the per-substep stepIndex latch (S2D_STEP_RELATCH): params.step_index = counter++,
@@ -106,6 +107,8 @@ struct SpecArgs {
   const float2* tw;
   int stochastic;       // force_amp > 0
   int* err;             // device error word (bounded waits that gave up)
+  int* row_nz;          // non-null: per row, 1 if the written PA/PB row holds a nonzero value;
+                        // a CTA whose rows are all zero then skips its transforms and stores
 };
 
 // rows held by the 2*PPB row slots of tile `tile`: pair p = rows (p, N-p); pair 0 = rows (0, N/2)
@@ -134,11 +137,24 @@ __device__ __forceinline__ float phys_cols_tile(const PhysArgs& a, int tile, flo
   float2* const bufs[2] = {smem + g * LDS, smem + (GA + g) * LDS};
 
   float2 v[2][V];
+  if (a.row_nz) {
+    // rows the row kernel left unwritten (all zero) are not read
+    int nz[V];
 #pragma unroll
-  for (int m = 0; m < V; ++m) {
-    const size_t o = (size_t)(t + T * m) * N + x;
-    v[0][m] = __ldcs(a.pa + o);
-    v[1][m] = __ldcs(a.pb + o);
+    for (int m = 0; m < V; ++m) nz[m] = __ldg(a.row_nz + t + T * m);
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const size_t o = (size_t)(t + T * m) * N + x;
+      v[0][m] = nz[m] ? __ldcs(a.pa + o) : make_float2(0.f, 0.f);
+      v[1][m] = nz[m] ? __ldcs(a.pb + o) : make_float2(0.f, 0.f);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const size_t o = (size_t)(t + T * m) * N + x;
+      v[0][m] = __ldcs(a.pa + o);
+      v[1][m] = __ldcs(a.pb + o);
+    }
   }
   fft_lines<N, V, +1, 2>(v, bufs, t, a.tw, CtaSync{});
   // v[0][m] = (omega, u), v[1][m].x = v at physical row y = t + T*m
@@ -301,6 +317,13 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
 
   if constexpr (TU::PREFETCH) mbar_wait_bounded(bar, parity, a.err, 1);
 
+  // per-row "holds a nonzero value" flags of this tile (only when the caller tracks them)
+  __shared__ int s_nz[32];
+  if (a.row_nz) {
+    if (t == 0) s_nz[slot] = 0;
+    __syncthreads();
+  }
+  bool row_nonzero = false;
   // RK3 stage update, one cell per iteration (kept rolled: the forcing and
   // integrating-factor code appears once in the kernel, not 16 times); the state
   // (and pointer-force) values of the next cell are loaded one iteration ahead so
@@ -352,7 +375,16 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
         a.wout[o] = w;
       }
       own1[PL::pad(c)] = w;
+      row_nonzero |= (w.x != 0.f || w.y != 0.f);
     }
+  }
+  if (a.row_nz) {
+    if (row_nonzero) s_nz[slot] = 1;
+    // all rows of the tile zero: their packs are zero -- flag them and skip the transforms
+    // and stores (the column kernels read no flagged row)
+    const int any = __syncthreads_or(row_nonzero ? 1 : 0);
+    if (t == 0) a.row_nz[row] = s_nz[slot];
+    if (!any) return;
   }
 
   // next-stage packs, scaled by the 1/N^2 of the inverse 2D transform, x-IFFT each;

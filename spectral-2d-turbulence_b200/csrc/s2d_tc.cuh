@@ -478,9 +478,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, cons
   const float2* src = (g < kTcCols ? a.pa : a.pb) + x0 + (g & (kTcCols - 1));
   float2 v[32];
   float mx = 0.f;
+  int nz[32];
+#pragma unroll
+  for (int n2 = 0; n2 < 32; ++n2) nz[n2] = a.row_nz ? __ldg(a.row_nz + t + 32 * n2) : 1;
 #pragma unroll
   for (int n2 = 0; n2 < 32; ++n2) {
-    v[n2] = __ldcs(src + (size_t)(t + 32 * n2) * N);
+    v[n2] = nz[n2] ? __ldcs(src + (size_t)(t + 32 * n2) * N) : make_float2(0.f, 0.f);   // flagged rows are zero
     mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
   }
   tc_setup<true, MODE != 0>(sm, m, tab);

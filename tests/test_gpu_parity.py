@@ -574,3 +574,34 @@ def test_relatch_equals_configure_per_substep(pkg):
             s.destroy()
     assert np.array_equal(outs[0], outs[1])
     assert np.array_equal(outs[0], outs[2])
+
+
+def test_skipped_zero_rows_read_back_as_zero(pkg):
+    """The row kernel leaves pack rows that are entirely zero unwritten (and flags them for
+    the column kernels); any other reader sees them as zeros.  Garbage written into the
+    packs beforehand must not survive into getBuffer or into the step."""
+    n = 256
+    ref = SpectralOracle(n=n, nu_h=1.0 / (n / 3.0) ** 8, hyper_p=4)
+    ref.set_vorticity(random_field(n, k0=20, seed=4, amplitude=5.0))       # dealiased
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=1.0, hyperP=4))
+        rng = np.random.default_rng(1)
+        junk = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+        s.setBuffer("packA", junk)
+        s.setBuffer("packB", junk)
+        load_state(s, w_in)
+        set_fixed_dt(s, 1e-3)
+        s.encodeStep()
+        ref.step(dt=1e-3)
+        assert rel_l2(current_state(s), ref.w) <= 1e-5
+        ky = np.fft.fftfreq(n, 1.0 / n)
+        out_rows = np.abs(ky) >= n / 3.0
+        for name in ("packA", "packB"):
+            p = s.getBuffer(name)
+            assert np.all(p[out_rows] == 0), name
+            assert np.any(p[~out_rows] != 0), name
+    finally:
+        s.destroy()
