@@ -170,6 +170,28 @@ int s2d_scenario_field(s2d_solver* s, int kind, double param, float* field_out);
  * solver.js:420-444), the field never leaving the device */
 int s2d_reset_scenario(s2d_solver* s, int kind, double param, int dye_pattern);
 
+/* ---------------------------------------------------------------- autotuner */
+/* No counterpart in the reference (its kernels have one fixed shape).  Each grid
+ * size registers up to S2D_TUNE_MAX launch shapes of the column and the row stage
+ * kernels (values per thread / radix of the line passes, resident CTAs per SM);
+ * s2d_autotune times them on this solver's own state (`steps` RK3 steps each, the
+ * state saved and restored around every trial), keeps the fastest column shape and
+ * then the fastest row shape with it, drops captured step graphs, and remembers the
+ * choice for later solvers of the same size, FFT precision and device.  Results
+ * differ from the default shape by FP32 rounding only. */
+#define S2D_TUNE_MAX 4
+typedef struct {
+  int32_t phys_variants, spec_variants;   /* registered column / row shapes */
+  int32_t phys_choice, spec_choice;       /* the shapes now in use */
+  float phys_us[S2D_TUNE_MAX];            /* device time per RK3 step with each column shape */
+  float spec_us[S2D_TUNE_MAX];            /* ... with each row shape (chosen column shape) */
+} s2d_tune_report;
+int s2d_autotune(s2d_solver* s, int steps, s2d_tune_report* report);
+/* use registered shapes `phys` (column kernel) and `spec` (row kernel) from now on */
+int s2d_tune_select(s2d_solver* s, int phys, int spec);
+/* the name of registered shape `index` of the column (kind 0) or row (kind 1) kernel */
+int s2d_tune_variant_name(s2d_solver* s, int kind, int index, char* out, int cap);
+
 /* ---------------------------------------------------------------- headless image */
 /* Renderer.render(encoder, solver, cfg) (render.js:63-87, render.wgsl:81-103) into a
  * host buffer of height*width RGBA8 pixels, row 0 at the top, instead of a canvas:

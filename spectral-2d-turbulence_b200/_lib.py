@@ -57,6 +57,15 @@ class s2d_splat(C.Structure):
                 ("dye_amp", C.c_float)]
 
 
+S2D_TUNE_MAX = 4
+
+
+class s2d_tune_report(C.Structure):
+    _fields_ = [("phys_variants", C.c_int32), ("spec_variants", C.c_int32), ("phys_choice", C.c_int32),
+                ("spec_choice", C.c_int32), ("phys_us", C.c_float * S2D_TUNE_MAX),
+                ("spec_us", C.c_float * S2D_TUNE_MAX)]
+
+
 class s2d_info(C.Structure):
     _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("nbins", C.c_int32), ("phase", C.c_int32),
                 ("dye_parity", C.c_int32), ("step_index", C.c_uint32), ("primed", C.c_int32),
@@ -103,6 +112,9 @@ PROTOTYPES = {
     "s2d_scenario_field": (_i, [_vp, _i, _d, C.POINTER(_f)]),
     "s2d_reset_scenario": (_i, [_vp, _i, _d, _i]),
     "s2d_render": (_i, [_vp, _i, _f, _f, _f, _i, _i, _vp]),
+    "s2d_autotune": (_i, [_vp, _i, C.POINTER(s2d_tune_report)]),
+    "s2d_tune_variant_name": (_i, [_vp, _i, _i, C.c_char_p, _i]),
+    "s2d_tune_select": (_i, [_vp, _i, _i]),
     "s2d_encode_prime": (_i, [_vp]),
     "s2d_encode_step": (_i, [_vp]),
     "s2d_encode_dye": (_i, [_vp]),

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -167,6 +168,7 @@ struct s2d_solver {
   bool primed = false, packs_valid = false, reduced_valid = false, disposed = false;
   int read_state = 0;  // 0 idle, 1 copied
   bool latch_pending = false;   // S2D_STEP_RELATCH: the next step's first column kernel latches
+  int phys_choice = 0, spec_choice = 0;   // stage-kernel shapes in use (ops->phys / ops->spec)
   std::map<GraphKey, GraphEntry> graphs;
   // instrumentation: event pairs around launches, by kernel class
   bool profiling = false;
@@ -174,6 +176,22 @@ struct s2d_solver {
   double prof_ms[S2D_PROF_CLASSES] = {0};
   int prof_cnt[S2D_PROF_CLASSES] = {0};
 };
+
+// Stage-kernel shapes chosen by s2d_autotune, per (device, n, FFT precision), shared by
+// the solvers created afterwards in this process.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
+static void tuned_choice(s2d_solver* s) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find(std::make_tuple(s->dev, s->n, s->fft_precision));
+  if (it == g_tuned.end()) return;
+  if (it->second.first < s->ops->n_phys) s->phys_choice = it->second.first;
+  if (it->second.second < s->ops->n_spec) s->spec_choice = it->second.second;
+}
+static void remember_choice(s2d_solver* s) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[std::make_tuple(s->dev, s->n, s->fft_precision)] = std::make_pair(s->phys_choice, s->spec_choice);
+}
 
 // RAII event pair around the launches of one kernel class (when profiling).
 // Inside stream capture the records must be external to become event-record
@@ -352,6 +370,7 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   s->nbins = n / 2 + 1;
   s->fft_precision = fft_precision;
   s->ops = ops;
+  tuned_choice(s);
   const size_t cbytes = (size_t)n * n * sizeof(float2);
   const size_t dbytes = (size_t)s->m * s->m * sizeof(ushort4);
   auto bail = [&](cudaError_t e, const char* what) {
@@ -374,7 +393,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMalloc(&s->vel, cbytes), "vel");
   TRY(cudaMalloc(&s->tw, sizeof(float2) * n), "twiddles");
   TRY(cudaMalloc(&s->dtbuf, sizeof(float) * 4), "dt");
-  const int nparts = std::max(std::max(ops->a_grid, 256), seed_parts_count(n));
+  // column-kernel grids are at most n CTAs in every registered shape
+  const int nparts = std::max(std::max(n, 256), seed_parts_count(n));
   TRY(cudaMalloc(&s->partials, sizeof(float) * nparts), "partials");
   TRY(cudaMalloc(&s->ticket, sizeof(unsigned)), "ticket");
   TRY(cudaMalloc(&s->row_nz, sizeof(int) * n), "row flags");
@@ -393,7 +413,7 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMallocHost(&s->h_fixed, sizeof(uint32_t) * (s->nbins + 2)), "pinned fixed");
   TRY(cudaMallocHost(&s->h_zonal, sizeof(float) * n), "pinned zonal");
   TRY(cudaMallocHost(&s->h_dt, sizeof(float) * 4), "pinned dt");
-  TRY(ops->set_attrs(), "kernel attributes");
+  TRY(set_all_attrs(*ops), "kernel attributes");
   TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
   if (fft_precision == S2D_FFT_TC_F16) {
@@ -595,7 +615,7 @@ static int enqueue_pack_prime(s2d_solver* s) {
   a.tw = s->tw;
   a.err = s->err;
   a.row_nz = s->row_nz;
-  s->ops->spec_rows(-1, false, a, s->stream);
+  s->ops->spec[s->spec_choice].run(-1, false, a, s->stream);
   S2D_LAUNCHED();
   s->packs_flagged = true;
   s->packs_valid = true;
@@ -637,7 +657,7 @@ static void enqueue_phys_cols(s2d_solver* s, int mode, const PhysArgs& a) {
     else if (mode == 1) tc::k_phys_cols_tc<1><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
     else tc::k_phys_cols_tc<2><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
   } else {
-    s->ops->phys_cols(mode, a, s->stream);
+    s->ops->phys[s->phys_choice].run(mode, a, s->stream);
   }
 }
 
@@ -696,7 +716,7 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     a.stochastic = s->hp.force_amp > 0.f ? 1 : 0;
     a.err = s->err;
     a.row_nz = s->row_nz;
-    s->ops->spec_rows(st, ptr, a, s->stream);
+    s->ops->spec[s->spec_choice].run(st, ptr, a, s->stream);
     S2D_LAUNCHED();
     s->packs_flagged = true;
   }
@@ -1071,6 +1091,135 @@ extern "C" int s2d_render(s2d_solver* s, int mode, float exposure, float vort_sc
   S2D_LAUNCHED();
   S2D_CUDA(cudaMemcpyAsync(rgba_out, s->image, px * sizeof(uchar4), cudaMemcpyDeviceToHost, s->stream));
   S2D_CUDA(cudaStreamSynchronize(s->stream));
+  return S2D_OK;
+}
+
+// ------------------------------------------------------------------ autotuner
+static void drop_graphs(s2d_solver* s) {
+  for (auto& kv : s->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    for (auto& ev : kv.second.events) {
+      cudaEventDestroy(std::get<1>(ev));
+      cudaEventDestroy(std::get<2>(ev));
+    }
+  }
+  s->graphs.clear();
+}
+
+extern "C" int s2d_tune_variant_name(s2d_solver* s, int kind, int index, char* out, int cap) {
+  S2D_USE(s);
+  if (!out || cap <= 0) return fail(S2D_ERR_ARG, "output is null");
+  const int count = kind == 0 ? s->ops->n_phys : kind == 1 ? s->ops->n_spec : -1;
+  if (count < 0) return fail(S2D_ERR_ARG, "kind is 0 (column) or 1 (row)");
+  if (index < 0 || index >= count) return fail(S2D_ERR_ARG, "variant index out of range");
+  std::snprintf(out, (size_t)cap, "%s", kind == 0 ? s->ops->phys[index].name : s->ops->spec[index].name);
+  return S2D_OK;
+}
+
+extern "C" int s2d_tune_select(s2d_solver* s, int phys, int spec) {
+  S2D_USE(s);
+  if (phys < 0 || phys >= s->ops->n_phys || spec < 0 || spec >= s->ops->n_spec)
+    return fail(S2D_ERR_ARG, "variant index out of range");
+  DeviceGuard guard(s->dev);
+  s->phys_choice = phys;
+  s->spec_choice = spec;
+  drop_graphs(s);   // captured steps hold the previous shapes' kernels
+  return S2D_OK;
+}
+
+extern "C" int s2d_autotune(s2d_solver* s, int steps, s2d_tune_report* report) {
+  S2D_USE(s);
+  if (steps < 1 || steps > 1000) return fail(S2D_ERR_ARG, "steps must be in 1..1000");
+  DeviceGuard guard(s->dev);
+  if (!s->primed)
+    if (int rc = s2d_encode_prime(s)) return rc;
+  const size_t cbytes = (size_t)s->n * s->n * sizeof(float2);
+  // everything a trial changes: the state ring, the velocity, the dt slots, host counters
+  float2* saved = nullptr;
+  S2D_CUDA(cudaMalloc(&saved, 4 * cbytes + 64));
+  float* saved_dt = reinterpret_cast<float*>(saved + 4 * (cbytes / sizeof(float2)));
+  auto cp = [&](void* dst, const void* src, size_t b) {
+    return cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToDevice, s->stream);
+  };
+  cudaError_t ce = cudaSuccess;
+  for (int i = 0; i < 3 && ce == cudaSuccess; ++i) ce = cp(saved + i * (cbytes / sizeof(float2)), s->state[i], cbytes);
+  if (ce == cudaSuccess) ce = cp(saved + 3 * (cbytes / sizeof(float2)), s->vel, cbytes);
+  if (ce == cudaSuccess) ce = cp(saved_dt, s->dtbuf, 4 * sizeof(float));
+  const int phase = s->phase, slot = s->slot;
+  const uint32_t step_index = s->step_index;
+  const bool reduced_valid = s->reduced_valid;
+  auto restore = [&]() -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cp(s->state[i], saved + i * (cbytes / sizeof(float2)), cbytes);
+    if (e == cudaSuccess) e = cp(s->vel, saved + 3 * (cbytes / sizeof(float2)), cbytes);
+    if (e == cudaSuccess) e = cp(s->dtbuf, saved_dt, 4 * sizeof(float));
+    s->phase = phase;
+    s->slot = slot;
+    s->step_index = step_index;
+    s->reduced_valid = reduced_valid;
+    s->packs_valid = false;   // the packs are re-primed from the restored state
+    return e;
+  };
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  const bool was_profiling = s->profiling;
+  s->profiling = false;
+  int rc = ce == cudaSuccess ? S2D_OK : fail(S2D_ERR_CUDA, std::string("autotune setup: ") + cudaGetErrorString(ce));
+  // one trial: restore, two untimed steps, then `steps` timed steps (step + fused CFL)
+  auto trial = [&](float* us) -> int {
+    if (cudaError_t e = restore(); e != cudaSuccess) return fail(S2D_ERR_CUDA, cudaGetErrorString(e));
+    for (int k = 0; k < 2 + steps; ++k) {
+      if (k == 2 && cudaEventRecord(e0, s->stream) != cudaSuccess) return fail(S2D_ERR_CUDA, "event");
+      if (int r = s2d_encode_step(s)) return r;
+      if (int r = s2d_encode_reduce(s)) return r;
+    }
+    if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+      return fail(S2D_ERR_CUDA, "event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *us = 1e3f * ms / steps;
+    return S2D_OK;
+  };
+  s2d_tune_report rep{};
+  rep.phys_variants = s->ops->n_phys;
+  rep.spec_variants = s->ops->n_spec;
+  const int p0 = s->phys_choice, q0 = s->spec_choice;
+  // the tensor-core column stage has one shape: only the row shapes are tuned there
+  const bool tc = s->fft_precision == S2D_FFT_TC_F16;
+  int best_p = p0, best_q = q0;
+  if (!rc) {
+    float best = 1e30f;
+    for (int i = 0; i < s->ops->n_phys && !rc; ++i) {
+      if (tc && i != p0) { rep.phys_us[i] = 0.f; continue; }
+      s->phys_choice = i;
+      rc = trial(&rep.phys_us[i]);
+      if (!rc && rep.phys_us[i] < best) { best = rep.phys_us[i]; best_p = i; }
+    }
+    s->phys_choice = best_p;
+    best = 1e30f;
+    for (int j = 0; j < s->ops->n_spec && !rc; ++j) {
+      s->spec_choice = j;
+      rc = trial(&rep.spec_us[j]);
+      if (!rc && rep.spec_us[j] < best) { best = rep.spec_us[j]; best_q = j; }
+    }
+  }
+  s->phys_choice = rc ? p0 : best_p;
+  s->spec_choice = rc ? q0 : best_q;
+  const cudaError_t re = restore();
+  cudaStreamSynchronize(s->stream);
+  cudaFree(saved);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  s->profiling = was_profiling;
+  drop_graphs(s);
+  if (rc) return rc;
+  if (re != cudaSuccess) return fail(S2D_ERR_CUDA, std::string("autotune restore: ") + cudaGetErrorString(re));
+  remember_choice(s);
+  rep.phys_choice = s->phys_choice;
+  rep.spec_choice = s->spec_choice;
+  if (report) *report = rep;
   return S2D_OK;
 }
 

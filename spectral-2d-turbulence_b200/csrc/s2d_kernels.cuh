@@ -25,9 +25,14 @@
 
 namespace s2d {
 
-template <int N_> struct Tune {
+// Launch shape of the stage kernels for N x N: V values per thread (T = N/V threads per
+// line; the line FFT runs radix-V passes), GA columns per column-kernel CTA, PPB row pairs
+// per row-kernel CTA, and the resident CTAs the register budget must allow (AMB_/BMB_;
+// 0 = as many as 128 registers a thread give).  Tune<N> is the default shape; the
+// autotuner picks among the variants each size registers (s2d_ops.cuh).
+template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0> struct Tune {
   static constexpr int N = N_;
-  static constexpr int V = 16;
+  static constexpr int V = V_;
   static constexpr int T = N / V;
   using PL = LinePlan<N, V>;
   // physical-column kernel: GA columns per CTA, lanes run over columns first
@@ -42,9 +47,9 @@ template <int N_> struct Tune {
   static constexpr int B_LDS = PL::stride(T >= 16 ? 0 : T);
   static constexpr int B_GRID = (N / 2) / PPB;
   static constexpr float KCUT = (float)(N / 3.0);
-  // resident CTAs the register budget must allow (128 registers a thread)
-  static constexpr int A_MINB = 65536 / (A_THREADS * 128) > 0 ? 65536 / (A_THREADS * 128) : 1;
-  static constexpr int B_MINB = 65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1;
+  // resident CTAs the register budget must allow
+  static constexpr int A_MINB = AMB_ ? AMB_ : (65536 / (A_THREADS * 128) > 0 ? 65536 / (A_THREADS * 128) : 1);
+  static constexpr int B_MINB = BMB_ ? BMB_ : (65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1);
   static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
   static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
   // rows the spectral-row kernel can stage by TMA bulk copy (wcur, w0, pointer force)
@@ -112,8 +117,8 @@ struct SpecArgs {
 };
 
 // rows held by the 2*PPB row slots of tile `tile`: pair p = rows (p, N-p); pair 0 = rows (0, N/2)
-template <int N> __device__ __forceinline__ int spec_row_of(int tile, int slot) {
-  const int pair = tile * Tune<N>::PPB + (slot >> 1);
+template <int N, class TU = Tune<N>> __device__ __forceinline__ int spec_row_of(int tile, int slot) {
+  const int pair = tile * TU::PPB + (slot >> 1);
   const int which = slot & 1;
   return pair == 0 ? (which ? N / 2 : 0) : (which ? N - pair : pair);
 }
@@ -127,9 +132,8 @@ template <int MODE, bool PTR> __host__ __device__ constexpr int spec_stage_array
 // physical columns: MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage
 // (stage + velocity + speed)
 // one tile of GA columns; returns this thread's max |u|+|v| (MODE != 1)
-template <int N, int MODE>
+template <int N, int MODE, class TU = Tune<N>>
 __device__ __forceinline__ float phys_cols_tile(const PhysArgs& a, int tile, float2* smem) {
-  using TU = Tune<N>;
   constexpr int V = TU::V, T = TU::T, GA = TU::GA, LDS = TU::A_LDS;
   const int tid = threadIdx.x;
   const int g = tid % GA, t = tid / GA;
@@ -229,12 +233,11 @@ __device__ __forceinline__ void cols_speed_finalize(const PhysArgs& a, float spe
   }
 }
 
-template <int N, int MODE>
-__global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_cols(PhysArgs a) {
-  using TU = Tune<N>;
+template <int N, int MODE, class TU = Tune<N>>
+__global__ void __launch_bounds__(TU::A_THREADS, TU::A_MINB) k_phys_cols(PhysArgs a) {
   extern __shared__ float2 smem[];
   phys_latch(a);
-  const float speed = phys_cols_tile<N, MODE>(a, blockIdx.x, smem);
+  const float speed = phys_cols_tile<N, MODE, TU>(a, blockIdx.x, smem);
   if constexpr (MODE != 1) cols_speed_finalize<TU::A_THREADS>(a, speed);
 }
 
@@ -242,17 +245,16 @@ __global__ void __launch_bounds__(Tune<N>::A_THREADS, Tune<N>::A_MINB) k_phys_co
 // spectral row pairs: MODE -1 = prime (pack wcur only), 0/1/2 = RK stage
 // `bar` is an initialised mbarrier in shared memory whose next phase is `parity`
 // (one phase per call); it orders the TMA bulk copies of this tile's rows.
-template <int N, int MODE, bool PTR>
+template <int N, int MODE, bool PTR, class TU = Tune<N>>
 __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, float2* smem, uint64_t* bar,
                                                uint32_t parity) {
-  using TU = Tune<N>;
   constexpr int V = TU::V, T = TU::T, LDS = TU::B_LDS;
   constexpr float KCUT = TU::KCUT;
   constexpr int NARR = spec_stage_arrays<MODE, PTR>();
   const int tid = threadIdx.x;
   const int t = tid % T, slot = tid / T;
   const int pair = tile * TU::PPB + (slot >> 1);
-  const int row = spec_row_of<N>(tile, slot);
+  const int row = spec_row_of<N, TU>(tile, slot);
   const int pslot = pair == 0 ? slot : (slot ^ 1);
   float2* const stage = reinterpret_cast<float2*>(reinterpret_cast<char*>(smem) + TU::B_STAGE_OFF);
   if constexpr (TU::PREFETCH) {
@@ -261,7 +263,7 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
     if (tid == 0) {
       mbar_arrive_expect_tx(bar, (uint32_t)(NARR * TU::B_ROWS * N * sizeof(float2)));
       for (int s = 0; s < TU::B_ROWS; ++s) {
-        const size_t ro = (size_t)spec_row_of<N>(tile, s) * N;
+        const size_t ro = (size_t)spec_row_of<N, TU>(tile, s) * N;
         int k = 0;
         bulk_g2s(stage + (size_t)(k++ * TU::B_ROWS + s) * N, a.wcur + ro, N * sizeof(float2), bar);
         if constexpr (MODE >= 1) bulk_g2s(stage + (size_t)(k++ * TU::B_ROWS + s) * N, a.w0 + ro, N * sizeof(float2), bar);
@@ -417,8 +419,8 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
 }
 
 // initialise the tile barrier of a spectral-row CTA (all threads call; one initialises)
-template <int N> __device__ __forceinline__ uint64_t* spec_barrier_init(float2* smem) {
-  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + Tune<N>::B_BAR_OFF);
+template <int N, class TU = Tune<N>> __device__ __forceinline__ uint64_t* spec_barrier_init(float2* smem) {
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + TU::B_BAR_OFF);
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
@@ -427,11 +429,11 @@ template <int N> __device__ __forceinline__ uint64_t* spec_barrier_init(float2* 
   return bar;
 }
 
-template <int N, int MODE, bool PTR>
-__global__ void __launch_bounds__(Tune<N>::B_THREADS, Tune<N>::B_MINB) k_spec_rows(SpecArgs a) {
+template <int N, int MODE, bool PTR, class TU = Tune<N>>
+__global__ void __launch_bounds__(TU::B_THREADS, TU::B_MINB) k_spec_rows(SpecArgs a) {
   extern __shared__ __align__(16) float2 smem[];
-  uint64_t* bar = spec_barrier_init<N>(smem);
-  spec_rows_tile<N, MODE, PTR>(a, blockIdx.x, smem, bar, 0u);
+  uint64_t* bar = spec_barrier_init<N, TU>(smem);
+  spec_rows_tile<N, MODE, PTR, TU>(a, blockIdx.x, smem, bar, 0u);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -262,6 +262,26 @@ class Solver:
         from . import scenarios
         scenarios.reset(self, name, cfg, dyePattern)
 
+    def autotune(self, steps: int = 20) -> dict:
+        """Time every registered launch shape of the column and row stage kernels on this
+        solver's state (restored afterwards) and keep the fastest (no reference counterpart).
+        Returns {"column": [(shape, us per RK3 step), ...], "row": [...], "choice": {...}}."""
+        rep = L.s2d_tune_report()
+        L.call("s2d_autotune", self._use(), int(steps), C.byref(rep))
+
+        def name(kind, i):
+            buf = C.create_string_buffer(64)
+            L.call("s2d_tune_variant_name", self._h, kind, i, buf, 64)
+            return buf.value.decode()
+        col = [(name(0, i), float(rep.phys_us[i])) for i in range(rep.phys_variants)]
+        row = [(name(1, i), float(rep.spec_us[i])) for i in range(rep.spec_variants)]
+        return {"column": col, "row": row,
+                "choice": {"column": col[rep.phys_choice][0], "row": row[rep.spec_choice][0]}}
+
+    def tuneSelect(self, column: int, row: int):
+        """Use registered stage-kernel shapes `column` / `row` (indices of autotune's lists)."""
+        L.call("s2d_tune_select", self._use(), int(column), int(row))
+
     def render(self, cfg: dict | None = None, width: int | None = None, height: int | None = None):
         """Renderer.render(encoder, solver, cfg) (render.js:63-87) without a canvas: an
         (height, width, 4) uint8 RGBA image, row 0 at the top.  cfg keys: mode (render.js:4

@@ -1,0 +1,67 @@
+"""Stage-kernel shapes and the autotuner: every registered shape matches the FP64 oracle,
+autotuning leaves the solver's state untouched and later solvers reuse its choice."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_helpers import config, current_state, load_state, rate_for, set_fixed_dt
+from oracle.spectral_oracle import SpectralOracle, random_field
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [512, 1024])
+def test_every_registered_shape_matches_oracle(pkg, n):
+    beta, mu, p, dt = 10.0, 1e-2, 4, 1e-3
+    nu_h = 1.0 / (n / 3.0) ** 8
+    ref0 = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
+    ref0.set_vorticity(random_field(n, k0=n / 8, seed=n + 3, amplitude=8.0))
+    w_in = ref0.w.astype(np.complex64)
+    ref0.w = w_in.astype(np.complex128)
+    ref0.step(dt=dt)
+    want = ref0.w
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        rep = s.autotune(steps=3)
+        ncol, nrow = len(rep["column"]), len(rep["row"])
+        assert ncol >= 2 and nrow >= 2            # the V=8 shapes are registered at these sizes
+        s.configure(config(beta=beta, drag=mu, viscosity=rate_for(nu_h, n, p), hyperP=p))
+        for i in range(ncol):
+            for j in range(nrow):
+                s.tuneSelect(i, j)
+                load_state(s, w_in)
+                set_fixed_dt(s, dt)
+                s.encodeStep()
+                err = rel_l2(current_state(s), want)
+                assert err <= 1e-5, (rep["column"][i][0], rep["row"][j][0], err)
+    finally:
+        s.destroy()
+
+
+def test_autotune_restores_state_and_is_remembered(pkg):
+    n = 1024
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.configure(config(viscosity=1.0, hyperP=4, forceAmp=0.1, forceK=64.0, forceWidth=2.0, cfl=0.5,
+                           dtMax=1e-3))
+        s.reset({"k0": 14, "amplitude": 6, "seed": 1, "dyePattern": "none"})
+        s.step(2, dye=False, reduce=True)
+        before = (current_state(s), s.getBuffer("dt"), s.getBuffer("vel"), s.phase, s.stepIndex)
+        rep = s.autotune(steps=5)
+        after = (current_state(s), s.getBuffer("dt"), s.getBuffer("vel"), s.phase, s.stepIndex)
+        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+        assert np.array_equal(before[2], after[2]) and before[3:] == after[3:]
+        assert all(us > 0 for _, us in rep["column"]) and all(us > 0 for _, us in rep["row"])
+        best_row = min(rep["row"], key=lambda kv: kv[1])[0]
+        assert rep["choice"]["row"] == best_row
+        # stepping on with the chosen shapes
+        s.step(2, dye=False, reduce=True, graph=True)
+        assert np.all(np.isfinite(current_state(s)))
+    finally:
+        s.destroy()
+    s2 = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        again = s2.autotune(steps=1)          # a new solver starts from the remembered choice
+        assert again["choice"]["row"] in [name for name, _ in again["row"]]
+    finally:
+        s2.destroy()
