@@ -560,6 +560,7 @@ def run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_256, seed=1
     mine = inst[rank::world]
     e = pkg.Ensemble(mine, device=dev)
     e.seedBand(4.0, 12.0, rms=1.0)
+    tune = e.autotune(3)                  # persistent-kernel shapes (state restored)
     stream = torch.cuda.ExternalStream(e.stream, device=dev)
     e.step(6, graph=True)
     e.synchronize()
@@ -583,7 +584,7 @@ def run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_256, seed=1
     return {"instances": count_total, "sizes": {str(n): c for n, c in groups},
             "n": groups[0][0] if len(groups) == 1 else None, "ensemble_steps_per_s": ens_steps_per_s,
             "instance_steps_per_s": ens_steps_per_s * count_total, "ms_per_ensemble_step": ms / steps,
-            "achieved_gbs": gbs, "hbm_peak_gbs": hbm, "frac_of_hbm": gbs / hbm, "finite": ok,
+            "achieved_gbs": gbs, "hbm_peak_gbs": hbm, "frac_of_hbm": gbs / hbm, "finite": ok, "autotune": tune,
             "note": "232 N^2 algorithmic bytes per instance-step; per-instance nu, beta, drag; graph-replayed"}
 
 

@@ -319,6 +319,12 @@ int s2d_ensemble_get_state(s2d_ensemble* e, int index, float* spectrum /* n*n*2 
 int s2d_ensemble_step(s2d_ensemble* e, int steps, int use_graph);
 /* FP64 energy and enstrophy of every instance (arrays of `count`). */
 int s2d_ensemble_energy(s2d_ensemble* e, double* energy, double* enstrophy);
+/* The autotuner for an ensemble (no reference counterpart): times the registered
+ * resident-CTA shapes of the persistent column and row kernels over `steps` RK3 steps
+ * of this ensemble (its state saved and restored bit for bit), keeps the fastest, and
+ * drops captured step graphs.  The shapes differ in register allocation only. */
+int s2d_ensemble_autotune(s2d_ensemble* e, int steps, s2d_tune_report* report);
+int s2d_ensemble_tune_variant_name(s2d_ensemble* e, int kind, int index, char* out, int cap);
 
 #ifdef __cplusplus
 }

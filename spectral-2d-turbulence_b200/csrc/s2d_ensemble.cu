@@ -9,6 +9,7 @@
 // RK3 step (6 launches) is captured into a CUDA graph and replayed.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
@@ -76,7 +77,9 @@ struct Pools {
   float2 *pa, *pb, *z;
 };
 
-__global__ void __launch_bounds__(kEnsAThreads, 2)
+// MINB: resident CTAs per SM the register allocation must allow (a tuned choice)
+template <int MINB>
+__global__ void __launch_bounds__(kEnsAThreads, MINB)
     k_ens_phys(const EnsInst* __restrict__ inst, const int2* __restrict__ items, int nitems, Pools pool) {
   extern __shared__ float2 smem[];
   for (int k = blockIdx.x; k < nitems; k += gridDim.x) {
@@ -106,11 +109,12 @@ template <int N> __device__ __forceinline__ float2* ens_spec_base(float2* smem) 
   return reinterpret_cast<float2*>(reinterpret_cast<char*>(smem) + (kEnsBStageOff - Tune<N>::B_STAGE_OFF));
 }
 
-// Six resident CTAs per SM (80 registers, some spilled to L1): over the 0.8 GB of
-// pooled state the row pass waits on HBM, and more CTAs in flight hide more of it
-// (256 x 256^2: 761 -> 831 ensemble-steps/s against four CTAs at 128 registers).
-template <int MODE>
-__global__ void __launch_bounds__(kEnsBThreads, 6)
+// MINB: resident CTAs per SM the register allocation must allow.  Over pooled state far
+// larger than L2 the row pass waits on HBM, and more CTAs in flight hide more of it even
+// with some registers spilled to L1 (256 x 256^2: 761 -> 831 ensemble-steps/s going from
+// four CTAs at 128 registers to six at 80); s2d_ensemble_autotune picks per ensemble.
+template <int MODE, int MINB>
+__global__ void __launch_bounds__(kEnsBThreads, MINB)
     k_ens_spec(const EnsInst* __restrict__ inst, const int2* __restrict__ items, int nitems, Pools pool, int phase,
                int* err) {
   extern __shared__ __align__(16) float2 smem[];
@@ -146,6 +150,46 @@ __global__ void __launch_bounds__(kEnsBThreads, 6)
     }
     __syncthreads();
   }
+}
+
+// ---- launch-shape variants of the two persistent stage kernels (index 0 = default)
+constexpr int kEnsPhysMinb[] = {2, 3};      // resident CTAs per SM of each shape
+constexpr int kEnsSpecMinb[] = {6, 4, 5};
+constexpr int kEnsNPhys = 2, kEnsNSpec = 3;
+
+template <int MINB> cudaError_t ens_phys_attrs() {
+  return cudaFuncSetAttribute(k_ens_phys<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsASmem);
+}
+template <int MINB> cudaError_t ens_spec_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_ens_spec<-1, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<0, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<1, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<2, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  return e;
+}
+const void* ens_phys_fn(int v) {
+  return v == 1 ? (const void*)k_ens_phys<3> : (const void*)k_ens_phys<2>;
+}
+const void* ens_spec_fn(int v) {
+  return v == 1 ? (const void*)k_ens_spec<1, 4> : v == 2 ? (const void*)k_ens_spec<1, 5> : (const void*)k_ens_spec<1, 6>;
+}
+void ens_launch_phys(int v, int grid, cudaStream_t st, const EnsInst* inst, const int2* items, int nitems, Pools pool) {
+  if (v == 1) k_ens_phys<3><<<grid, kEnsAThreads, kEnsASmem, st>>>(inst, items, nitems, pool);
+  else k_ens_phys<2><<<grid, kEnsAThreads, kEnsASmem, st>>>(inst, items, nitems, pool);
+}
+template <int MODE>
+void ens_launch_spec_m(int v, int grid, cudaStream_t st, const EnsInst* inst, const int2* items, int nitems, Pools pool,
+                       int phase, int* err) {
+  if (v == 1) k_ens_spec<MODE, 4><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
+  else if (v == 2) k_ens_spec<MODE, 5><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
+  else k_ens_spec<MODE, 6><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
+}
+void ens_launch_spec(int mode, int v, int grid, cudaStream_t st, const EnsInst* inst, const int2* items, int nitems,
+                     Pools pool, int phase, int* err) {
+  if (mode < 0) ens_launch_spec_m<-1>(v, grid, st, inst, items, nitems, pool, phase, err);
+  else if (mode == 0) ens_launch_spec_m<0>(v, grid, st, inst, items, nitems, pool, phase, err);
+  else if (mode == 1) ens_launch_spec_m<1>(v, grid, st, inst, items, nitems, pool, phase, err);
+  else ens_launch_spec_m<2>(v, grid, st, inst, items, nitems, pool, phase, err);
 }
 
 __global__ void k_ens_twiddles(float2* tw, int n) {
@@ -223,7 +267,8 @@ struct s2d_ensemble {
   uint32_t* dseeds = nullptr;
   int2 *items_a = nullptr, *items_b = nullptr;
   int nitems_a = 0, nitems_b = 0;
-  int grid_a = 0, grid_b = 0;
+  int grid_a[kEnsNPhys] = {}, grid_b[kEnsNSpec] = {};   // persistent grids per launch shape
+  int pv = 0, sv = 0;                                   // launch shapes in use
   Pools pool{};
   float2* tw = nullptr;
   double* sums = nullptr;    // 2 * count
@@ -356,16 +401,21 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
   TRY(cudaMemcpyAsync(e->dseeds, e->seeds.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice, e->stream), "copy");
   TRY(cudaMemcpyAsync(e->items_a, ia.data(), sizeof(int2) * ia.size(), cudaMemcpyHostToDevice, e->stream), "copy");
   TRY(cudaMemcpyAsync(e->items_b, ib.data(), sizeof(int2) * ib.size(), cudaMemcpyHostToDevice, e->stream), "copy");
-  TRY(cudaFuncSetAttribute(k_ens_phys, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsASmem), "attr");
-  TRY(cudaFuncSetAttribute(k_ens_spec<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem), "attr");
-  TRY(cudaFuncSetAttribute(k_ens_spec<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem), "attr");
-  TRY(cudaFuncSetAttribute(k_ens_spec<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem), "attr");
-  TRY(cudaFuncSetAttribute(k_ens_spec<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem), "attr");
-  int occ_a = 0, occ_b = 0;
-  TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_ens_phys, kEnsAThreads, kEnsASmem), "occupancy");
-  TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_ens_spec<1>, kEnsBThreads, kEnsBSmem), "occupancy");
-  e->grid_a = std::min(e->nitems_a, std::max(1, occ_a) * prop.multiProcessorCount);
-  e->grid_b = std::min(e->nitems_b, std::max(1, occ_b) * prop.multiProcessorCount);
+  TRY(ens_phys_attrs<2>(), "attr");
+  TRY(ens_phys_attrs<3>(), "attr");
+  TRY(ens_spec_attrs<4>(), "attr");
+  TRY(ens_spec_attrs<5>(), "attr");
+  TRY(ens_spec_attrs<6>(), "attr");
+  for (int v = 0; v < kEnsNPhys; ++v) {
+    int occ = 0;
+    TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_phys_fn(v), kEnsAThreads, kEnsASmem), "occupancy");
+    e->grid_a[v] = std::min(e->nitems_a, std::max(1, occ) * prop.multiProcessorCount);
+  }
+  for (int v = 0; v < kEnsNSpec; ++v) {
+    int occ = 0;
+    TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_spec_fn(v), kEnsBThreads, kEnsBSmem), "occupancy");
+    e->grid_b[v] = std::min(e->nitems_b, std::max(1, occ) * prop.multiProcessorCount);
+  }
   TRY(cudaStreamSynchronize(e->stream), "sync");
 #undef TRY
   cudaSetDevice(prev);
@@ -451,11 +501,9 @@ extern "C" int s2d_ensemble_get_state(s2d_ensemble* e, int index, float* spectru
 static int ens_enqueue_step(s2d_ensemble* e) {
   const int p = e->phase;
   for (int st = 0; st < 3; ++st) {
-    k_ens_phys<<<e->grid_a, kEnsAThreads, kEnsASmem, e->stream>>>(e->dinst, e->items_a, e->nitems_a, e->pool);
+    ens_launch_phys(e->pv, e->grid_a[e->pv], e->stream, e->dinst, e->items_a, e->nitems_a, e->pool);
     E_LAUNCHED();
-    if (st == 0) k_ens_spec<0><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
-    else if (st == 1) k_ens_spec<1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
-    else k_ens_spec<2><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
+    ens_launch_spec(st, e->sv, e->grid_b[e->sv], e->stream, e->dinst, e->items_b, e->nitems_b, e->pool, p, e->err);
     E_LAUNCHED();
   }
   e->phase = (p + 1) % 3;
@@ -470,7 +518,8 @@ extern "C" int s2d_ensemble_step(s2d_ensemble* e, int steps, int use_graph) {
   if (prev != e->dev) cudaSetDevice(e->dev);
   int rc = S2D_OK;
   if (!e->packs_valid) {
-    k_ens_spec<-1><<<e->grid_b, kEnsBThreads, kEnsBSmem, e->stream>>>(e->dinst, e->items_b, e->nitems_b, e->pool, e->phase, e->err);
+    ens_launch_spec(-1, e->sv, e->grid_b[e->sv], e->stream, e->dinst, e->items_b, e->nitems_b, e->pool, e->phase,
+                    e->err);
     if (cudaGetLastError() != cudaSuccess) rc = efail(S2D_ERR_CUDA, "prime launch failed");
     e->packs_valid = true;
   }
@@ -509,6 +558,90 @@ extern "C" int s2d_ensemble_step(s2d_ensemble* e, int steps, int use_graph) {
   for (; !rc && done < steps; ++done) rc = ens_enqueue_step(e);
   if (prev != e->dev) cudaSetDevice(prev);
   return rc;
+}
+
+extern "C" int s2d_ensemble_tune_variant_name(s2d_ensemble* e, int kind, int index, char* out, int cap) {
+  E_USE(e);
+  if (!out || cap <= 0) return efail(S2D_ERR_ARG, "output is null");
+  const int count = kind == 0 ? kEnsNPhys : kind == 1 ? kEnsNSpec : -1;
+  if (count < 0 || index < 0 || index >= count) return efail(S2D_ERR_ARG, "variant out of range");
+  std::snprintf(out, (size_t)cap, "%d CTAs/SM", kind == 0 ? kEnsPhysMinb[index] : kEnsSpecMinb[index]);
+  return S2D_OK;
+}
+
+extern "C" int s2d_ensemble_autotune(s2d_ensemble* e, int steps, s2d_tune_report* report) {
+  E_USE(e);
+  if (steps < 1 || steps > 300) return efail(S2D_ERR_ARG, "steps must be in 1..300");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != e->dev) cudaSetDevice(e->dev);
+  const size_t cbytes = sizeof(float2) * (size_t)e->cells;
+  float2* saved = nullptr;
+  int rc = S2D_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&saved, 3 * cbytes) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess)
+    rc = efail(S2D_ERR_CUDA, "autotune: out of device memory for the saved state");
+  const int phase = e->phase;
+  auto restore = [&]() {
+    for (int i = 0; i < 3; ++i)
+      cudaMemcpyAsync(e->pool.s[i], saved + i * e->cells, cbytes, cudaMemcpyDeviceToDevice, e->stream);
+    e->phase = phase;
+    e->packs_valid = false;
+  };
+  if (!rc)
+    for (int i = 0; i < 3; ++i)
+      cudaMemcpyAsync(saved + i * e->cells, e->pool.s[i], cbytes, cudaMemcpyDeviceToDevice, e->stream);
+  auto trial = [&](float* us) -> int {
+    restore();
+    if (int r = s2d_ensemble_step(e, 1, 0)) return r;   // primes, one untimed step
+    cudaEventRecord(e0, e->stream);
+    if (int r = s2d_ensemble_step(e, steps, 0)) return r;
+    cudaEventRecord(e1, e->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return efail(S2D_ERR_CUDA, "autotune: event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *us = 1e3f * ms / steps;
+    return S2D_OK;
+  };
+  s2d_tune_report rep{};
+  rep.phys_variants = kEnsNPhys;
+  rep.spec_variants = kEnsNSpec;
+  const int pv0 = e->pv, sv0 = e->sv;
+  int best_p = pv0, best_s = sv0;
+  if (!rc) {
+    float best = 1e30f;
+    for (int v = 0; v < kEnsNPhys && !rc; ++v) {
+      e->pv = v;
+      rc = trial(&rep.phys_us[v]);
+      if (!rc && rep.phys_us[v] < best) { best = rep.phys_us[v]; best_p = v; }
+    }
+    e->pv = best_p;
+    best = 1e30f;
+    for (int v = 0; v < kEnsNSpec && !rc; ++v) {
+      e->sv = v;
+      rc = trial(&rep.spec_us[v]);
+      if (!rc && rep.spec_us[v] < best) { best = rep.spec_us[v]; best_s = v; }
+    }
+  }
+  e->pv = rc ? pv0 : best_p;
+  e->sv = rc ? sv0 : best_s;
+  if (saved) restore();
+  cudaStreamSynchronize(e->stream);
+  if (saved) cudaFree(saved);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (auto& kv : e->graphs) {          // captured with the previous shapes
+    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+  }
+  e->graphs.clear();
+  if (prev != e->dev) cudaSetDevice(prev);
+  if (rc) return rc;
+  rep.phys_choice = e->pv;
+  rep.spec_choice = e->sv;
+  if (report) *report = rep;
+  return S2D_OK;
 }
 
 extern "C" int s2d_ensemble_energy(s2d_ensemble* e, double* energy, double* enstrophy) {

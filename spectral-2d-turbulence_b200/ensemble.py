@@ -64,6 +64,21 @@ class Ensemble:
     def step(self, steps: int = 1, graph: bool = True):
         L.call("s2d_ensemble_step", self._h, int(steps), 1 if graph else 0)
 
+    def autotune(self, steps: int = 3) -> dict:
+        """Pick the resident-CTA shapes of the persistent stage kernels by timing them on
+        this ensemble (state restored afterwards); no reference counterpart."""
+        rep = L.s2d_tune_report()
+        L.call("s2d_ensemble_autotune", self._h, int(steps), C.byref(rep))
+
+        def name(kind, i):
+            buf = C.create_string_buffer(32)
+            L.call("s2d_ensemble_tune_variant_name", self._h, kind, i, buf, 32)
+            return buf.value.decode()
+        col = [(name(0, i), float(rep.phys_us[i])) for i in range(rep.phys_variants)]
+        row = [(name(1, i), float(rep.spec_us[i])) for i in range(rep.spec_variants)]
+        return {"column": col, "row": row,
+                "choice": {"column": col[rep.phys_choice][0], "row": row[rep.spec_choice][0]}}
+
     def synchronize(self):
         L.call("s2d_ensemble_synchronize", self._h)
 

@@ -65,3 +65,36 @@ def test_autotune_restores_state_and_is_remembered(pkg):
         assert again["choice"]["row"] in [name for name, _ in again["row"]]
     finally:
         s2.destroy()
+
+
+def _mixed_ensemble(pkg):
+    inst = []
+    for n, count in ((64, 3), (128, 2), (256, 2)):
+        for k in range(count):
+            inst.append({"n": n, "beta": 5.0 + k, "drag": 1e-2, "nuH": 5e-4, "hyperP": 1, "dt": 2e-3,
+                         "seed": len(inst)})
+    e = pkg.Ensemble(inst)
+    e.seedBand(4.0, 12.0, rms=1.0)
+    return e
+
+
+def test_ensemble_autotune_restores_state_and_matches(pkg):
+    e = _mixed_ensemble(pkg)
+    ref = _mixed_ensemble(pkg)
+    try:
+        e.step(2, graph=False)
+        ref.step(2, graph=False)
+        before = [e.getState(i) for i in range(e.count)]
+        rep = e.autotune(2)
+        assert len(rep["column"]) == 2 and len(rep["row"]) == 3
+        assert all(us > 0 for _, us in rep["column"] + rep["row"])
+        for i in range(e.count):
+            assert np.array_equal(e.getState(i), before[i])
+        e.step(6, graph=True)
+        ref.step(6, graph=True)
+        for i in range(e.count):
+            a, b = e.getState(i), ref.getState(i)
+            assert rel_l2(a, b) <= 1e-6, i
+    finally:
+        e.destroy()
+        ref.destroy()
