@@ -484,12 +484,12 @@ def _bench_solver(pkg, dev, fft, seed):
     return s
 
 
-def tc_divergence(pkg, dev, steps=10):
-    """rel L2 between the FP32 and the tensor-core step after 1 and `steps` steps of the
+def tc_divergence(pkg, dev, steps=10, fft_tc="tc-f16"):
+    """rel L2 between the FP32 and a tensor-core step after 1 and `steps` steps of the
     benchmark configuration from the same seeded state (adaptive dt, forcing on)."""
     import numpy as np
     out = {}
-    for fft in ("fp32", "tc-f16"):
+    for fft in ("fp32", fft_tc):
         s = _bench_solver(pkg, dev, fft, 1)
         try:
             s.step(1, dye=False, reduce=True, graph=False)
@@ -502,8 +502,8 @@ def tc_divergence(pkg, dev, steps=10):
 
     def rel(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    return {"1_step": rel(out["tc-f16"][0], out["fp32"][0]),
-            f"{steps}_steps": rel(out["tc-f16"][1], out["fp32"][1])}
+    return {"1_step": rel(out[fft_tc][0], out["fp32"][0]),
+            f"{steps}_steps": rel(out[fft_tc][1], out["fp32"][1])}
 
 
 def run_tc_leg(pkg, torch, world, rank, dev, args, fp32_value, fp32_rk3):
@@ -528,7 +528,18 @@ def run_tc_leg(pkg, torch, world, rank, dev, args, fp32_value, fp32_rk3):
     solver.destroy()
     value = world * args.steps / (ms / 1e3)
     rk3 = world * args.steps / (ms_rk3 / 1e3)
+    # the BF16 split (16 significant bits per operand): speed and drift from FP32
+    bsolver = _bench_solver(pkg, dev, "tc-bf16", 1 + rank)
+    bstream = torch.cuda.ExternalStream(bsolver.stream, device=dev)
+    bsolver.autotune(5)
+    bsolver.step(max(args.warmup, 6), dye=False, reduce=True, graph=True, relatch=True)
+    bsolver.synchronize()
+    ms_bf16 = max_over_ranks(_timed_steps(bsolver, bstream, torch, args.steps, False), world)
+    bsolver.destroy()
+    bf16 = {"rk3_only_steps_per_s": world * args.steps / (ms_bf16 / 1e3),
+            "rel_l2_vs_fp32": tc_divergence(pkg, dev, fft_tc="tc-bf16")}
     return {"fft": "split FP16 hi+lo tcgen05 DFT-GEMM (y-transforms); FP32 row transforms",
+            "bf16_split": bf16,
             "steps_per_s": value, "rk3_only_steps_per_s": rk3,
             "fp32_steps_per_s": fp32_value, "fp32_rk3_only_steps_per_s": fp32_rk3,
             "rk3_speedup_vs_fp32": rk3 / fp32_rk3, "speedup_vs_fp32": value / fp32_value,

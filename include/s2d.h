@@ -63,8 +63,9 @@ enum s2d_buffer_id {
 
 /* FFT arithmetic of the fused step */
 #define S2D_FFT_FP32 0            /* CUDA-core FP32 FFT */
-#define S2D_FFT_TC_F16 1          /* tensor-core DFT-GEMM, FP16 hi+lo split, FP32 accumulate */
-#define S2D_FFT_TC_BF16 2         /* tensor-core DFT-GEMM, BF16 hi+mid+lo split, FP32 accumulate */
+#define S2D_FFT_TC_F16 1          /* tensor-core DFT-GEMM, FP16 hi+lo split, FP32 accumulate (N = 1024) */
+#define S2D_FFT_TC_BF16 2         /* tensor-core DFT-GEMM, BF16 hi+lo split, FP32 accumulate (N = 1024):
+                                     16 significant bits per operand (the FP16 split keeps 22) */
 
 /* dye patterns of paintDye (solver.js:446-473) */
 #define S2D_DYE_NONE 0

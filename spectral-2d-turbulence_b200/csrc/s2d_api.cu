@@ -348,6 +348,38 @@ extern "C" int s2d_dealias_mask_table(int n, uint8_t* out) {
 }
 
 // ------------------------------------------------------------------ lifecycle
+// ------------------------------------------------------------------ tensor-core kernels by precision
+template <class P> static cudaError_t tc_attrs() {
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
+  const int smem = tc::kTcSmem;
+  chk(cudaFuncSetAttribute(tc::k_fft_tc<0, -1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  chk(cudaFuncSetAttribute(tc::k_fft_tc<0, +1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  chk(cudaFuncSetAttribute(tc::k_fft_tc<1, -1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  chk(cudaFuncSetAttribute(tc::k_fft_tc<1, +1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<0, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<2, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
+  return e;
+}
+template <class P> static void tc_fft2_launch(float2* buf, int sign, const char* tab, int* err, cudaStream_t st) {
+  const dim3 g(1024 / tc::kTcLines), b(tc::kTcThreads);
+  if (sign < 0) {
+    tc::k_fft_tc<0, -1, P><<<g, b, tc::kTcSmem, st>>>(buf, tab, err);
+    tc::k_fft_tc<1, -1, P><<<g, b, tc::kTcSmem, st>>>(buf, tab, err);
+  } else {
+    tc::k_fft_tc<0, +1, P><<<g, b, tc::kTcSmem, st>>>(buf, tab, err);
+    tc::k_fft_tc<1, +1, P><<<g, b, tc::kTcSmem, st>>>(buf, tab, err);
+  }
+}
+template <class P> static void tc_cols_launch(int mode, const PhysArgs& a, const char* tab, int* err, cudaStream_t st) {
+  const dim3 g(tc::kTcColsGrid), b(tc::kTcThreads);
+  if (mode == 0) tc::k_phys_cols_tc<0, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
+  else if (mode == 1) tc::k_phys_cols_tc<1, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
+  else tc::k_phys_cols_tc<2, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
+}
+static bool is_tc(const s2d_solver* s) { return s->fft_precision != S2D_FFT_FP32; }
+
 extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s2d_solver** out) {
   if (!out) return fail(S2D_ERR_ARG, "out is null");
   *out = nullptr;
@@ -356,9 +388,9 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   const NOps* ops = ops_for(n);
   if (!ops) return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " outside 32..4096");
   if (dye_scale < 1 || dye_scale > 4) return fail(S2D_ERR_ARG, "dye_scale must be 1..4");
-  if (fft_precision != S2D_FFT_FP32 && fft_precision != S2D_FFT_TC_F16)
-    return fail(S2D_ERR_ARG, "unknown or unsupported FFT arithmetic (S2D_FFT_FP32, S2D_FFT_TC_F16)");
-  if (fft_precision == S2D_FFT_TC_F16 && n != 1024)
+  if (fft_precision != S2D_FFT_FP32 && fft_precision != S2D_FFT_TC_F16 && fft_precision != S2D_FFT_TC_BF16)
+    return fail(S2D_ERR_ARG, "unknown FFT arithmetic (S2D_FFT_FP32, S2D_FFT_TC_F16, S2D_FFT_TC_BF16)");
+  if (fft_precision != S2D_FFT_FP32 && n != 1024)
     return fail(S2D_ERR_UNSUPPORTED_N, "the tensor-core FFT is built for N = 1024");
   if (int rc = check_device(device)) return rc;
   DeviceGuard guard(device);
@@ -416,18 +448,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(set_all_attrs(*ops), "kernel attributes");
   TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
-  if (fft_precision == S2D_FFT_TC_F16) {
-    TRY(cudaFuncSetAttribute(tc::k_fft_tc<0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
-    TRY(cudaFuncSetAttribute(tc::k_fft_tc<0, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
-    TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
-    TRY(cudaFuncSetAttribute(tc::k_fft_tc<1, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcSmem), "tc");
-    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
-        "tc");
-    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
-        "tc");
-    TRY(cudaFuncSetAttribute(tc::k_phys_cols_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem),
-        "tc");
-  }
+  if (fft_precision == S2D_FFT_TC_F16) TRY(tc_attrs<tc::PrecF16>(), "tensor-core kernel attributes");
+  if (fft_precision == S2D_FFT_TC_BF16) TRY(tc_attrs<tc::PrecBF16>(), "tensor-core kernel attributes");
   // zero everything the reference's fresh buffers hold as zero
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
   TRY(cudaMemsetAsync(s->packA, 0, cbytes, s->stream), "memset");
@@ -442,9 +464,10 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream), "memset");
   k_twiddles<<<(n + 255) / 256, 256, 0, s->stream>>>(s->tw, n);
   TRY(cudaGetLastError(), "twiddle kernel");
-  if (fft_precision == S2D_FFT_TC_F16) {
+  if (fft_precision != S2D_FFT_FP32) {
     TRY(cudaMalloc(&s->tctab, tc::kTabBytes), "tensor-core tables");
-    tc::k_tc_tables<<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
+    if (fft_precision == S2D_FFT_TC_BF16) tc::k_tc_tables<tc::PrecBF16><<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
+    else tc::k_tc_tables<tc::PrecF16><<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
     TRY(cudaGetLastError(), "tensor-core table kernel");
   }
   // an unconfigured solver has all-zero parameters apart from the grid constants
@@ -580,18 +603,10 @@ extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
 static inline unsigned cells_grid(int n) { return (unsigned)(((size_t)n * n + 255) / 256); }
 
 static int enqueue_fft2(s2d_solver* s, float2* buf, int sign) {
-  if (s->fft_precision == S2D_FFT_TC_F16) {
+  if (is_tc(s)) {
     // tensor-core DFT-GEMM passes, 8 lines of 1024 per CTA
-    const dim3 g(1024 / tc::kTcLines), b(tc::kTcThreads);
-    if (sign < 0) {
-      tc::k_fft_tc<0, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
-      S2D_LAUNCHED();
-      tc::k_fft_tc<1, -1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
-    } else {
-      tc::k_fft_tc<0, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
-      S2D_LAUNCHED();
-      tc::k_fft_tc<1, +1><<<g, b, tc::kTcSmem, s->stream>>>(buf, s->tctab, s->err);
-    }
+    if (s->fft_precision == S2D_FFT_TC_BF16) tc_fft2_launch<tc::PrecBF16>(buf, sign, s->tctab, s->err, s->stream);
+    else tc_fft2_launch<tc::PrecF16>(buf, sign, s->tctab, s->err, s->stream);
     S2D_LAUNCHED();
     return S2D_OK;
   }
@@ -649,13 +664,11 @@ static PhysArgs phys_args(s2d_solver* s, int reduce) {
 }
 
 // the physical-column stage: tensor-core y-transforms when the solver was created
-// with S2D_FFT_TC_F16 (1024^2 only), else the FP32 whole-line kernel
+// with S2D_FFT_TC_F16 / S2D_FFT_TC_BF16 (1024^2 only), else the FP32 whole-line kernel
 static void enqueue_phys_cols(s2d_solver* s, int mode, const PhysArgs& a) {
-  if (s->fft_precision == S2D_FFT_TC_F16) {
-    const dim3 g(tc::kTcColsGrid), b(tc::kTcThreads);
-    if (mode == 0) tc::k_phys_cols_tc<0><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
-    else if (mode == 1) tc::k_phys_cols_tc<1><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
-    else tc::k_phys_cols_tc<2><<<g, b, tc::kTcColsSmem, s->stream>>>(a, s->tctab, s->err);
+  if (is_tc(s)) {
+    if (s->fft_precision == S2D_FFT_TC_BF16) tc_cols_launch<tc::PrecBF16>(mode, a, s->tctab, s->err, s->stream);
+    else tc_cols_launch<tc::PrecF16>(mode, a, s->tctab, s->err, s->stream);
   } else {
     s->ops->phys[s->phys_choice].run(mode, a, s->stream);
   }
@@ -1187,7 +1200,7 @@ extern "C" int s2d_autotune(s2d_solver* s, int steps, s2d_tune_report* report) {
   rep.spec_variants = s->ops->n_spec;
   const int p0 = s->phys_choice, q0 = s->spec_choice;
   // the tensor-core column stage has one shape: only the row shapes are tuned there
-  const bool tc = s->fft_precision == S2D_FFT_TC_F16;
+  const bool tc = is_tc(s);
   int best_p = p0, best_q = q0;
   if (!rc) {
     float best = 1e30f;

@@ -9,7 +9,8 @@
 // inputs as 64 interleaved (re, im) values along K; B is the real block form of
 // the 32 x 32 DFT matrix.  The interleaved row order makes every operand store of
 // a warp land in distinct shared-memory banks.
-// Operands are FP16 split as hi + lo with x ~= hi + lo and the three products
+// Operands are split as hi + lo in FP16 (or BF16, the PrecBF16 instantiation) with
+// x ~= hi + lo and the three products
 // hi.hi + hi.lo + lo.hi accumulated in FP32 in tensor memory (TMEM).  A per-CTA
 // power-of-two scale keeps the first GEMM's operand inside FP16 range; the
 // second GEMM's operand is bounded by 32 x the first (|Y| <= sum |x|), so it
@@ -21,6 +22,7 @@
 // SBO = 1024 B between M-adjacent core matrices), tcgen05.commit arrives on an
 // mbarrier, and every warp reads its 32 TMEM lanes back with tcgen05.ld.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include "s2d_async.cuh"
 #include "s2d_device.cuh"
@@ -84,9 +86,24 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 // instruction descriptor: FP16 x FP16 -> FP32, A and B K-major, M x N
-__host__ __device__ constexpr uint32_t idesc_f16(int m, int n) {
-  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+// fmt: operand format of A and B (0 = FP16, 1 = BF16), bits [7,10) and [10,13)
+__host__ __device__ constexpr uint32_t idesc_f16(int m, int n, uint32_t fmt = 0) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
+
+// operand precision of the split: a pair type, its format code, pack and unpack
+struct PrecF16 {
+  using H2 = __half2;
+  static constexpr uint32_t kFmt = 0;
+  __device__ __forceinline__ static H2 pack(float a, float b) { return __floats2half2_rn(a, b); }
+  __device__ __forceinline__ static float2 unpack(H2 v) { return __half22float2(v); }
+};
+struct PrecBF16 {
+  using H2 = __nv_bfloat162;
+  static constexpr uint32_t kFmt = 1;
+  __device__ __forceinline__ static H2 pack(float a, float b) { return __floats2bfloat162_rn(a, b); }
+  __device__ __forceinline__ static float2 unpack(H2 v) { return __bfloat1622float2(v); }
+};
 
 // ------------------------------------------------------------------ operand layout
 constexpr int kK = 64;                  // real K of a DFT32 (32 complex inputs)
@@ -100,50 +117,53 @@ __device__ __forceinline__ uint32_t op_off(int r, int k) {
   return (uint32_t)((r >> 3) * kSBO + (k >> 3) * kLBO + (r & 7) * 16 + (k & 7) * 2);
 }
 
-// split x into hi + lo (FP16) with x ~= hi + lo
-__device__ __forceinline__ void split2(float re, float im, __half2& hi, __half2& lo) {
-  hi = __floats2half2_rn(re, im);
-  const float2 h = __half22float2(hi);
-  lo = __floats2half2_rn(re - h.x, im - h.y);
+// split x into hi + lo with x ~= hi + lo
+template <class P>
+__device__ __forceinline__ void split2(float re, float im, typename P::H2& hi, typename P::H2& lo) {
+  hi = P::pack(re, im);
+  const float2 h = P::unpack(hi);
+  lo = P::pack(re - h.x, im - h.y);
 }
 // store complex (re, im) at row r, complex column j (K = 2j, 2j+1) of the hi and lo planes
+template <class P>
 __device__ __forceinline__ void put_c(char* hi_plane, char* lo_plane, int r, int j, float re, float im) {
-  __half2 h, l;
-  split2(re, im, h, l);
+  typename P::H2 h, l;
+  split2<P>(re, im, h, l);
   const uint32_t o = op_off(r, 2 * j);
-  *reinterpret_cast<__half2*>(hi_plane + o) = h;
-  *reinterpret_cast<__half2*>(lo_plane + o) = l;
+  *reinterpret_cast<typename P::H2*>(hi_plane + o) = h;
+  *reinterpret_cast<typename P::H2*>(lo_plane + o) = l;
 }
 
 // Real block form of the 32-point DFT with sign SIGN, stored transposed (row = output
 // real index n, K = input real index): for output k2 and input n2, W = c + i s,
 //   Bt[2k2][2n2] = c, Bt[2k2][2n2+1] = -s, Bt[2k2+1][2n2] = s, Bt[2k2+1][2n2+1] = c.
 // W_32^{n2 k2} = W_1024^{32 n2 k2} from the FP64-generated twiddle table (forward sign).
-template <int SIGN>
+template <int SIGN, class P>
 __device__ __forceinline__ void build_dft32(char* hi_plane, char* lo_plane, const float2* __restrict__ tw1024) {
   for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
     const int k2 = e >> 5, n2 = e & 31;
     float2 w = __ldg(tw1024 + ((32 * n2 * k2) & 1023));
     if (SIGN > 0) w.y = -w.y;
     const float c = w.x, s = w.y;
-    __half2 h, l;
+    typename P::H2 h, l;
     // row 2k2: (c, -s) at K = 2n2, 2n2+1
-    split2(c, -s, h, l);
+    split2<P>(c, -s, h, l);
     uint32_t o = op_off(2 * k2, 2 * n2);
-    *reinterpret_cast<__half2*>(hi_plane + o) = h;
-    *reinterpret_cast<__half2*>(lo_plane + o) = l;
+    *reinterpret_cast<typename P::H2*>(hi_plane + o) = h;
+    *reinterpret_cast<typename P::H2*>(lo_plane + o) = l;
     // row 2k2+1: (s, c)
-    split2(s, c, h, l);
+    split2<P>(s, c, h, l);
     o = op_off(2 * k2 + 1, 2 * n2);
-    *reinterpret_cast<__half2*>(hi_plane + o) = h;
-    *reinterpret_cast<__half2*>(lo_plane + o) = l;
+    *reinterpret_cast<typename P::H2*>(hi_plane + o) = h;
+    *reinterpret_cast<typename P::H2*>(lo_plane + o) = l;
   }
 }
 
 // D(block b) = A(block b) . B over K = 64: hi.hi + hi.lo + lo.hi, 3 x 4 MMAs of K = 16
+template <class P>
 __device__ __forceinline__ void issue_dft_gemm(uint32_t tmem_d, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
                                                uint32_t b_lo) {
-  constexpr uint32_t idesc = idesc_f16(128, 64);
+  constexpr uint32_t idesc = idesc_f16(128, 64, P::kFmt);
   uint32_t acc = 0;
 #pragma unroll
   for (int kb = 0; kb < 4; ++kb) {
@@ -200,9 +220,10 @@ constexpr int kTabFwd = 2 * kBBytes;
 constexpr int kTabTw = 4 * kBBytes;
 constexpr int kTabBytes = kTabTw + kTcTwBytes;
 
+template <class P>
 __global__ void k_tc_tables(char* tab, const float2* __restrict__ tw1024) {
-  build_dft32<+1>(tab + kTabInv, tab + kTabInv + kBBytes, tw1024);
-  build_dft32<-1>(tab + kTabFwd, tab + kTabFwd + kBBytes, tw1024);
+  build_dft32<+1, P>(tab + kTabInv, tab + kTabInv + kBBytes, tw1024);
+  build_dft32<-1, P>(tab + kTabFwd, tab + kTabFwd + kBBytes, tw1024);
   float2* t = reinterpret_cast<float2*>(tab + kTabTw);
   for (int e = threadIdx.x; e < 32 * kTcTwLd; e += blockDim.x) {
     const int n1 = e / kTcTwLd, k2 = e - n1 * kTcTwLd;
@@ -256,17 +277,18 @@ __device__ __forceinline__ float cta_max_slots(const float* red) {
   return m;
 }
 
-__device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+template <class H2> __device__ __forceinline__ uint32_t h2bits(H2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
 // four consecutive complex K values (one 16-byte core-matrix row) of operand row r,
 // starting at complex index 4*kc, scaled by s, split into the hi and lo planes
+template <class P>
 __device__ __forceinline__ void put_c4(char* hi_plane, char* lo_plane, int r, int kc, float2 a, float2 b, float2 c,
                                        float2 d, float s) {
-  __half2 h0, h1, h2, h3, l0, l1, l2, l3;
-  split2(a.x * s, a.y * s, h0, l0);
-  split2(b.x * s, b.y * s, h1, l1);
-  split2(c.x * s, c.y * s, h2, l2);
-  split2(d.x * s, d.y * s, h3, l3);
+  typename P::H2 h0, h1, h2, h3, l0, l1, l2, l3;
+  split2<P>(a.x * s, a.y * s, h0, l0);
+  split2<P>(b.x * s, b.y * s, h1, l1);
+  split2<P>(c.x * s, c.y * s, h2, l2);
+  split2<P>(d.x * s, d.y * s, h3, l3);
   const uint32_t o = op_off(r, 8 * kc);
   *reinterpret_cast<uint4*>(hi_plane + o) = make_uint4(h2bits(h0), h2bits(h1), h2bits(h2), h2bits(h3));
   *reinterpret_cast<uint4*>(lo_plane + o) = make_uint4(h2bits(l0), h2bits(l1), h2bits(l2), h2bits(l3));
@@ -305,17 +327,18 @@ __device__ __forceinline__ void tmem_read(uint32_t addr, float (&y)[2 * NC]) {
   tmem_wait_ld();
 }
 
+template <class P>
 __device__ __forceinline__ void issue_blocks(int nb, uint32_t tmem, uint32_t base, int bhi, int blo) {
-  issue_dft_gemm(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
+  issue_dft_gemm<P>(tmem, base + kTcAHi, base + kTcALo, base + bhi, base + blo);
   if (nb == 2)
-    issue_dft_gemm(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
+    issue_dft_gemm<P>(tmem + 64, base + kTcAHi + kBlockBytes, base + kTcALo + kBlockBytes, base + bhi, base + blo);
 }
 
 // Both DFT32 GEMMs of the 1024-point four-step transform of L lines whose step-A
 // operand (row n1 * L + line, K = n2: x[n1 + 32 n2] * scale) the caller has written.
 // On return the thread's TcGeom row is (k2 = index, line) and x[j] = X[k2 + 32 (col0 + j)],
 // unscaled.  The barrier's next parity is `phase`; two phases are consumed.
-template <int SIGN, int L>
+template <int SIGN, int L, class P>
 __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t* bar, uint32_t phase, float scale,
                                               int* err, float2 (&x)[TcGeom<L>::NC]) {
   using G = TcGeom<L>;
@@ -328,7 +351,7 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
   __syncthreads();
   if (threadIdx.x == 0) {
     fence_after_sync();
-    issue_blocks(G::NB, tmem, base, bhi, blo);
+    issue_blocks<P>(G::NB, tmem, base, bhi, blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase, err, 2);
@@ -351,7 +374,7 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
       const float wx = e ? t4.z : t4.x, wy = SIGN > 0 ? -(e ? t4.w : t4.y) : (e ? t4.w : t4.y);
       const float re = (y[2 * (j + e)] * wx - y[2 * (j + e) + 1] * wy) * 0.03125f;
       const float im = (y[2 * (j + e)] * wy + y[2 * (j + e) + 1] * wx) * 0.03125f;
-      put_c(a_hi, a_lo, k2 * L + line, n1, re, im);
+      put_c<P>(a_hi, a_lo, k2 * L + line, n1, re, im);
     }
   }
   fence_proxy_async();
@@ -359,7 +382,7 @@ __device__ __forceinline__ void fft1024_gemms(char* sm, uint32_t tmem, uint64_t*
   __syncthreads();
   if (threadIdx.x == 0) {
     fence_after_sync();
-    issue_blocks(G::NB, tmem, base, bhi, blo);
+    issue_blocks<P>(G::NB, tmem, base, bhi, blo);
     mma_commit(bar);
   }
   mbar_wait_bounded(bar, phase ^ 1u, err, 3);
@@ -387,7 +410,7 @@ constexpr int kTcLines = 8;
 constexpr int kTcRowLd = 1024 + 4;                // padded staging line (rows pass)
 static_assert(kTcLines * kTcRowLd * 8 <= kTcMisc, "row staging must fit below the misc words");
 
-template <int AXIS, int SIGN>
+template <int AXIS, int SIGN, class P = PrecF16>
 __global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const char* __restrict__ tab, int* err) {
   constexpr int N = 1024;
   extern __shared__ __align__(1024) char sm[];
@@ -411,11 +434,11 @@ __global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const char*
   const uint32_t tmem = *m.tslot;
 #pragma unroll
   for (int kc = 0; kc < 8; ++kc)
-    put_c4(sm + kTcAHi, sm + kTcALo, t * kTcLines + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3],
-           scale);
+    put_c4<P>(sm + kTcAHi, sm + kTcALo, t * kTcLines + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2],
+              v[4 * kc + 3], scale);
   tc_wait_tables(m, err);
   float2 x[32];
-  fft1024_gemms<SIGN, 8>(sm, tmem, m.bar, 0u, scale, err, x);
+  fft1024_gemms<SIGN, 8, P>(sm, tmem, m.bar, 0u, scale, err, x);
   const float post = SIGN > 0 ? 1.f / N : 1.f;
   // thread: line = lane & 7, k2; X[k2 + 32 k1] in x[k1].  Stage (over the dead operands)
   // for coalesced stores.
@@ -465,7 +488,7 @@ __device__ __forceinline__ float2* vel_stage_slot(char* sm, int y, int col) {
   return reinterpret_cast<float2*>(base) + cols_stage_idx(y & 511, col);
 }
 
-template <int MODE>
+template <int MODE, class P = PrecF16>
 __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, const char* __restrict__ tab, int* err) {
   constexpr int N = 1024;
   extern __shared__ __align__(1024) char sm[];
@@ -493,10 +516,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, cons
   const uint32_t tmem = *m.tslot;
 #pragma unroll
   for (int kc = 0; kc < 8; ++kc)
-    put_c4(sm + kTcAHi, sm + kTcALo, t * 8 + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3], scale);
+    put_c4<P>(sm + kTcAHi, sm + kTcALo, t * 8 + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3], scale);
   tc_wait_tables(m, err);
   float2 x[32];
-  fft1024_gemms<+1, 8>(sm, tmem, m.bar, 0u, scale, err, x);
+  fft1024_gemms<+1, 8, P>(sm, tmem, m.bar, 0u, scale, err, x);
   // thread: line = lane & 7 (PA column c = line & 3 for line < 4, PB column for line >= 4),
   // k2 = TcGeom<8>::index(); x[k1] at y = k2 + 32 k1.  The partner line is lane ^ 4.
   const bool is_pa = (lane & 4) == 0;
@@ -531,10 +554,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, cons
     for (int q = 0; q < 4; ++q) {
       const float2 z0 = is_pa ? x[4 * q] : x[16 + 4 * q], z1 = is_pa ? x[4 * q + 1] : x[16 + 4 * q + 1];
       const float2 z2 = is_pa ? x[4 * q + 2] : x[16 + 4 * q + 2], z3 = is_pa ? x[4 * q + 3] : x[16 + 4 * q + 3];
-      put_c4(sm + kTcAHi, sm + kTcALo, k2 * 4 + c, is_pa ? q : 4 + q, z0, z1, z2, z3, scale_z);
+      put_c4<P>(sm + kTcAHi, sm + kTcALo, k2 * 4 + c, is_pa ? q : 4 + q, z0, z1, z2, z3, scale_z);
     }
     float2 zf[16];
-    fft1024_gemms<-1, 4>(sm, tmem, m.bar, 0u, scale_z, err, zf);
+    fft1024_gemms<-1, 4, P>(sm, tmem, m.bar, 0u, scale_z, err, zf);
     // thread: column c' = lane & 3, k2' = TcGeom<4>::index(); Z(ky = k2' + 32 (col0 + j))
     using G4 = TcGeom<4>;
     const int cz = G4::line(), kz = G4::index(), c0 = G4::col0();

@@ -439,9 +439,47 @@ def test_tc_fft2_matches_numpy(pkg):
 
 
 def test_tc_precision_only_at_1024(pkg):
-    with pytest.raises(pkg.S2DError) as ei:
-        pkg.Solver.create(n=512, fft="tc-f16")
-    assert ei.value.status == -2
+    for fft in ("tc-f16", "tc-bf16"):
+        with pytest.raises(pkg.S2DError) as ei:
+            pkg.Solver.create(n=512, fft=fft)
+        assert ei.value.status == -2
+
+
+def test_precision_sweep_fft_and_step(pkg):
+    """FP32, FP16-split and BF16-split FFT paths at 1024^2 against FP64: 2D FFT and one
+    fused step (rel L2, printed).  FP32 and the FP16 split meet 1e-5; the BF16 split keeps
+    16 significant bits per operand (the FP16 split 22), so its error is larger."""
+    n, dt = 1024, 1e-3
+    rng = np.random.default_rng(3)
+    a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    fa = np.fft.fft2(a.astype(np.complex128))
+    nu_h = 1.0 / (n / 3.0) ** 8
+    ref = SpectralOracle(n=n, beta=10.0, mu=1e-2, nu_h=nu_h, hyper_p=4)
+    ref.set_vorticity(random_field(n, k0=n / 8, seed=21, amplitude=8.0))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    ref.step(dt=dt)
+    errs = {}
+    for fft in ("fp32", "tc-f16", "tc-bf16"):
+        s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+        try:
+            s.setBuffer("packB", a)
+            s.fft.forward(None, "packB")
+            e_fft = rel_l2(s.getBuffer("packB"), fa)
+            s.configure(config(beta=10.0, drag=1e-2, viscosity=rate_for(nu_h, n, 4), hyperP=4))
+            load_state(s, w_in)
+            set_fixed_dt(s, dt)
+            s.setSplats([])
+            s.encodeStep()
+            e_step = rel_l2(current_state(s), ref.w)
+        finally:
+            s.destroy()
+        errs[fft] = (e_fft, e_step)
+        print(f"{fft}: 2D FFT rel L2 {e_fft:.3e}, one step rel L2 {e_step:.3e}")
+    assert errs["fp32"][0] <= 1e-5 and errs["fp32"][1] <= 1e-5
+    assert errs["tc-f16"][0] <= 1e-5 and errs["tc-f16"][1] <= 1e-5
+    assert errs["tc-bf16"][0] <= 1e-3 and errs["tc-bf16"][1] <= 1e-3
+    assert errs["tc-bf16"][0] > errs["tc-f16"][0]
 
 
 def _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt):
