@@ -249,9 +249,26 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([float(x)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard_by_cost(instances, world):
+    """Split ensemble instances over `world` ranks with balanced cost N^2 log2 N (greedy,
+    largest first into the least-loaded rank; ties to the lower rank) -- deterministic, so
+    every rank computes the same partition without communicating."""
+    import math
+    order = sorted(range(len(instances)), key=lambda i: (-instances[i]["n"], i))
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for i in order:
+        n = instances[i]["n"]
+        r = min(range(world), key=lambda k: (load[k], k))
+        shards[r].append(instances[i])
+        load[r] += n * n * math.log2(n)
+    return shards
 
 
 # ------------------------------------------------------------------ CPU reference arm
@@ -568,7 +585,7 @@ def run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_256, seed=1
             inst.append({"n": n, "beta": float(rng.uniform(0, 20)), "drag": float(rng.uniform(0, 2e-2)),
                          "nuH": float(rng.uniform(1e-4, 1e-3)), "hyperP": 1, "dt": 2e-3, "seed": len(inst)})
     count_total = len(inst)
-    mine = inst[rank::world]
+    mine = shard_by_cost(inst, world)[rank]
     e = pkg.Ensemble(mine, device=dev)
     e.seedBand(4.0, 12.0, rms=1.0)
     tune = e.autotune(3)                  # persistent-kernel shapes (state restored)
