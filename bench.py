@@ -346,8 +346,9 @@ def run_ours(args):
     solver.reset({"k0": 14, "amplitude": 0, "seed": 1, "dyePattern": "bands"})
     solver.seedBand(4.0, 12.0, rms=1.0, seed=1 + rank)
     stream = torch.cuda.ExternalStream(solver.stream, device=dev)
-    # stage-kernel launch shapes chosen by the library's autotuner (before any timing)
-    tune = solver.autotune(20)
+    # stage-kernel launch shapes chosen by the library's autotuner (before any timing), or
+    # pinned with --shapes (reproducible profiling)
+    tune = pinned_shapes(solver, args.shapes) if args.shapes else solver.autotune(20)
 
     # warm-up (also captures the graphs of the 6 (phase, dt slot, dye parity) combinations)
     solver.step(max(args.warmup, 6), dye=True, reduce=True, graph=True, relatch=True)
@@ -482,6 +483,13 @@ def run_ours(args):
     return 0
 
 
+def pinned_shapes(solver, spec):
+    """--shapes C,R: use column shape C and row shape R (indices of Solver.autotune()'s lists)."""
+    c, r = (int(v) for v in spec.split(","))
+    solver.tuneSelect(c, r)
+    return {"pinned": {"column": c, "row": r}}
+
+
 def _timed_steps(solver, stream, torch, steps, dye):
     solver.step(3, dye=dye, reduce=True, graph=True, relatch=True)
     solver.synchronize()
@@ -529,7 +537,7 @@ def run_tc_leg(pkg, torch, world, rank, dev, args, fp32_value, fp32_rk3):
     drifts from the FP32 step."""
     solver = _bench_solver(pkg, dev, "tc-f16", 1 + rank)
     stream = torch.cuda.ExternalStream(solver.stream, device=dev)
-    tune = solver.autotune(20)
+    tune = pinned_shapes(solver, args.shapes) if args.shapes else solver.autotune(20)
     solver.step(max(args.warmup, 6), dye=True, reduce=True, graph=True, relatch=True)
     solver.synchronize()
     barrier(world)
@@ -548,7 +556,10 @@ def run_tc_leg(pkg, torch, world, rank, dev, args, fp32_value, fp32_rk3):
     # the BF16 split (16 significant bits per operand): speed and drift from FP32
     bsolver = _bench_solver(pkg, dev, "tc-bf16", 1 + rank)
     bstream = torch.cuda.ExternalStream(bsolver.stream, device=dev)
-    bsolver.autotune(5)
+    if args.shapes:
+        pinned_shapes(bsolver, args.shapes)
+    else:
+        bsolver.autotune(5)
     bsolver.step(max(args.warmup, 6), dye=False, reduce=True, graph=True, relatch=True)
     bsolver.synchronize()
     ms_bf16 = max_over_ranks(_timed_steps(bsolver, bstream, torch, args.steps, False), world)
@@ -625,6 +636,8 @@ def main(argv=None):
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tc", action="store_true")
+    ap.add_argument("--shapes", default=None,
+                    help="C,R: pin the stage-kernel shapes (column C, row R) instead of autotuning")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
