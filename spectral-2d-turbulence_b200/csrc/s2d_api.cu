@@ -128,6 +128,14 @@ struct GraphEntry {
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> events;
 };
 
+static size_t diag_block_bytes(int nbins, int n) {
+  return (sizeof(double) + sizeof(uint32_t)) * (size_t)(nbins + 2) + sizeof(float) * (size_t)n;
+}
+
+constexpr int kUploadSlots = 8;
+constexpr size_t kUploadSlotBytes = 512;
+static_assert(sizeof(DevParams) <= kUploadSlotBytes && sizeof(DevSplats) <= kUploadSlotBytes, "upload slot");
+
 struct s2d_solver {
   int dev = 0, n = 0, m = 0, nbins = 0, dye_scale = 1, fft_precision = 0;
   cudaStream_t stream = nullptr;
@@ -140,9 +148,11 @@ struct s2d_solver {
   unsigned* ticket = nullptr;
   DevParams* dparams = nullptr;
   DevSplats* dsplats = nullptr;
-  double* diag = nullptr;      // nbins + 2
-  uint32_t* diag_fixed = nullptr;
-  float* zonal = nullptr;
+  // diagnostics block, one allocation (one clear, one readback copy): FP64 bins + totals
+  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n]
+  double* diag = nullptr;
+  uint32_t* diag_fixed = nullptr;   // inside diag's allocation
+  float* zonal = nullptr;           // inside diag's allocation
   double* seed_parts = nullptr;
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
   int* err = nullptr;                 // device error word (bounded waits that gave up)
@@ -152,12 +162,17 @@ struct s2d_solver {
   uchar4* image = nullptr;            // headless render target, grown on demand
   size_t image_px = 0;
   ushort4* dye[3] = {nullptr, nullptr, nullptr};
-  // pinned readback staging (copyDiagnostics)
+  // pinned readback staging (copyDiagnostics), laid out as the device block
   double* h_diag = nullptr;
-  uint32_t* h_fixed = nullptr;
-  float* h_zonal = nullptr;
+  uint32_t* h_fixed = nullptr;      // inside h_diag's allocation
+  float* h_zonal = nullptr;         // inside h_diag's allocation
   float* h_dt = nullptr;
   cudaEvent_t diag_event = nullptr;
+  // pinned upload ring for the per-step parameter and splat blocks: slot i is rewritten
+  // only after the copy that last read it has run (upload_ev[i])
+  char* h_upload = nullptr;
+  cudaEvent_t upload_ev[kUploadSlots] = {};
+  int upload_next = 0;
   // host mirror of the JS Solver fields
   DevParams hp{};
   DevSplats hs{};
@@ -237,14 +252,30 @@ static void free_solver(s2d_solver* s) {
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
                       s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->diag_fixed, s->zonal, s->seed_parts, s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
+                      s->diag, s->seed_parts, s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
-  void* host_ptrs[] = {s->h_diag, s->h_fixed, s->h_zonal, s->h_dt};
+  void* host_ptrs[] = {s->h_diag, s->h_dt, s->h_upload};
   for (void* p : host_ptrs)
     if (p) cudaFreeHost(p);
   if (s->diag_event) cudaEventDestroy(s->diag_event);
+  for (cudaEvent_t ev : s->upload_ev)
+    if (ev) cudaEventDestroy(ev);
   if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// host -> device copy of a small per-step block through the pinned upload ring; the
+// source may be reused as soon as this returns
+static cudaError_t upload(s2d_solver* s, void* dst, const void* src, size_t bytes) {
+  const int i = s->upload_next;
+  s->upload_next = (i + 1) % kUploadSlots;
+  cudaError_t e = cudaEventSynchronize(s->upload_ev[i]);   // the copy that last read slot i
+  if (e != cudaSuccess) return e;
+  char* slot = s->h_upload + (size_t)i * kUploadSlotBytes;
+  std::memcpy(slot, src, bytes);
+  e = cudaMemcpyAsync(dst, slot, bytes, cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) return e;
+  return cudaEventRecord(s->upload_ev[i], s->stream);
 }
 
 #define S2D_USE(s)                                                         \
@@ -432,19 +463,21 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMalloc(&s->row_nz, sizeof(int) * n), "row flags");
   TRY(cudaMalloc(&s->dparams, sizeof(DevParams)), "params");
   TRY(cudaMalloc(&s->dsplats, sizeof(DevSplats)), "splats");
-  TRY(cudaMalloc(&s->diag, sizeof(double) * (s->nbins + 2)), "diag");
-  TRY(cudaMalloc(&s->diag_fixed, sizeof(uint32_t) * (s->nbins + 2)), "diag fixed");
-  TRY(cudaMalloc(&s->zonal, sizeof(float) * n), "zonal");
+  TRY(cudaMalloc(&s->diag, diag_block_bytes(s->nbins, n)), "diag");
+  s->diag_fixed = reinterpret_cast<uint32_t*>(s->diag + s->nbins + 2);
+  s->zonal = reinterpret_cast<float*>(s->diag_fixed + s->nbins + 2);
   TRY(cudaMalloc(&s->seed_parts, sizeof(double) * seed_parts_count(n)), "seed partials");
   TRY(cudaMalloc(&s->step_counter, sizeof(uint32_t)), "step counter");
   TRY(cudaMalloc(&s->err, sizeof(int)), "error word");
   TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream), "memset");
   TRY(cudaMemsetAsync(s->step_counter, 0, sizeof(uint32_t), s->stream), "memset");
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
-  TRY(cudaMallocHost(&s->h_diag, sizeof(double) * (s->nbins + 2)), "pinned diag");
-  TRY(cudaMallocHost(&s->h_fixed, sizeof(uint32_t) * (s->nbins + 2)), "pinned fixed");
-  TRY(cudaMallocHost(&s->h_zonal, sizeof(float) * n), "pinned zonal");
+  TRY(cudaMallocHost(&s->h_diag, diag_block_bytes(s->nbins, n)), "pinned diag");
+  s->h_fixed = reinterpret_cast<uint32_t*>(s->h_diag + s->nbins + 2);
+  s->h_zonal = reinterpret_cast<float*>(s->h_fixed + s->nbins + 2);
   TRY(cudaMallocHost(&s->h_dt, sizeof(float) * 4), "pinned dt");
+  TRY(cudaMallocHost(&s->h_upload, kUploadSlotBytes * kUploadSlots), "pinned upload ring");
+  for (cudaEvent_t& ev : s->upload_ev) TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
   TRY(set_all_attrs(*ops), "kernel attributes");
   TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
@@ -477,8 +510,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   s->hp.force_norm = (float)(0.01 * n * n);
   s->hp.dx = (float)(2.0 * M_PI / n);
   s->hs = DevSplats{};
-  TRY(cudaMemcpyAsync(s->dparams, &s->hp, sizeof(DevParams), cudaMemcpyHostToDevice, s->stream), "params");
-  TRY(cudaMemcpyAsync(s->dsplats, &s->hs, sizeof(DevSplats), cudaMemcpyHostToDevice, s->stream), "splats");
+  TRY(upload(s, s->dparams, &s->hp, sizeof(DevParams)), "params");
+  TRY(upload(s, s->dsplats, &s->hs, sizeof(DevSplats)), "splats");
   TRY(cudaStreamSynchronize(s->stream), "create sync");
 #undef TRY
   *out = s;
@@ -576,7 +609,7 @@ extern "C" int s2d_configure(s2d_solver* s, const s2d_params* p) {
   h.kcut = (float)kcut;
   h.force_norm = (float)(0.01 * s->n * s->n);
   h.n = s->n;
-  S2D_CUDA(cudaMemcpyAsync(s->dparams, &h, sizeof(DevParams), cudaMemcpyHostToDevice, s->stream));
+  S2D_CUDA(upload(s, s->dparams, &h, sizeof(DevParams)));
   s->configured = true;
   return S2D_OK;
 }
@@ -595,7 +628,7 @@ extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
     d.r = a.color[0]; d.g = a.color[1]; d.b = a.color[2];
     d.radius = a.radius; d.amp = a.amp; d.dye_amp = a.dye_amp;
   }
-  S2D_CUDA(cudaMemcpyAsync(s->dsplats, &s->hs, sizeof(DevSplats), cudaMemcpyHostToDevice, s->stream));
+  S2D_CUDA(upload(s, s->dsplats, &s->hs, sizeof(DevSplats)));
   return S2D_OK;
 }
 
@@ -793,8 +826,8 @@ extern "C" int s2d_encode_reduce(s2d_solver* s) {
 }
 
 static int sync_step_counter(s2d_solver* s) {
-  const uint32_t v = s->step_index;   // pageable source: staged before the call returns
-  S2D_CUDA(cudaMemcpyAsync(s->step_counter, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+  const uint32_t v = s->step_index;
+  S2D_CUDA(upload(s, s->step_counter, &v, sizeof(v)));
   return S2D_OK;
 }
 
@@ -905,13 +938,10 @@ extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
   const int n = s->n, nb = s->nbins;
-  S2D_CUDA(cudaMemsetAsync(s->diag, 0, sizeof(double) * (nb + 2), s->stream));
-  S2D_CUDA(cudaMemsetAsync(s->diag_fixed, 0, sizeof(uint32_t) * (nb + 2), s->stream));
-  const unsigned items = (unsigned)((size_t)n * n / kDiagCells);
-  const unsigned blocks = std::min<unsigned>((items + 255) / 256, 148u * 4u);
-  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->diag, s->diag_fixed, n);
-  S2D_LAUNCHED();
-  k_zonal_mean<<<n, 128, 0, s->stream>>>(s->vel, s->zonal, n);
+  S2D_CUDA(cudaMemsetAsync(s->diag, 0, (sizeof(double) + sizeof(uint32_t)) * (nb + 2), s->stream));
+  const unsigned blocks = (unsigned)(diag_tiles(n) + diag_zonal_ctas(n));
+  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->vel, s->diag, s->diag_fixed,
+                                                            s->zonal, n);
   S2D_LAUNCHED();
   return S2D_OK;
 }
@@ -921,10 +951,7 @@ extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
   if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
   DeviceGuard guard(s->dev);
   const int nb = s->nbins;
-  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, sizeof(double) * (nb + 2), cudaMemcpyDeviceToHost, s->stream));
-  S2D_CUDA(cudaMemcpyAsync(s->h_fixed, s->diag_fixed, sizeof(uint32_t) * (nb + 2), cudaMemcpyDeviceToHost,
-                           s->stream));
-  S2D_CUDA(cudaMemcpyAsync(s->h_zonal, s->zonal, sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->stream));
+  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, diag_block_bytes(nb, s->n), cudaMemcpyDeviceToHost, s->stream));
   S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), sizeof(float) * 2, cudaMemcpyDeviceToHost, s->stream));
   S2D_CUDA(cudaEventRecord(s->diag_event, s->stream));
   s->read_state = 1;

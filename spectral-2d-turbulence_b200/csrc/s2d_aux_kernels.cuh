@@ -215,17 +215,46 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 // ------------------------------------------------------------------ diagnostics
 // Both spectra in one pass over the state: the FP64 radial spectrum, energy and
 // enstrophy (spectral2d.py:92-104) and the reference's u32 fixed-point bins,
-// truncating, in the dealias band (spectrum.wgsl:19-39).  A thread takes 8
-// consecutive cells of a row, whose |k| bins
-// change slowly along kx, and adds each run of equal bins once (shared-memory bins
-// per CTA, one global atomic per bin per CTA); totals are warp-reduced.  The u32
-// sums wrap mod 2^32 in any order, so the fixed-point result equals the per-cell
-// atomics bit for bit.
+// truncating, in the dealias band (spectrum.wgsl:19-39); the zonal mean of u
+// (spectrum.wgsl:41-68) in the same launch.
+//
+// A CTA takes a k-space tile of TW x TH cells (TW = min(64, n), TW * TH = 2048), so the
+// cells it sees span only ~|tile diagonal| radial bins and it flushes a few dozen bins
+// to global memory instead of all n/2 + 1.  A thread takes 8 consecutive cells of a row,
+// whose bins change slowly along kx, and adds each run of equal bins once (shared-memory
+// bins per CTA, one global atomic per nonzero bin per CTA); totals are warp-reduced.  The
+// u32 sums wrap mod 2^32 in any order, so the fixed-point result equals the per-cell
+// atomics bit for bit.  CTAs past the tiles take the zonal mean, one warp per row.
+//
+// Per cell: the f32 bin round(sqrtf(k2)) is the reference's; the FP64 bin
+// floor(sqrt(k2) + 0.5) is the same integer corrected by one step with integer tests
+// (b^2 - b < k2 <= b^2 + b; sqrt(k2) is never a half-integer).  n^4 is a power of two,
+// so scaling by its reciprocal is the division, bit for bit.
 constexpr int kDiagCells = 8;
+__host__ __device__ constexpr int diag_tile_w(int n) { return n < 64 ? n : 64; }
+__host__ __device__ constexpr int diag_tile_h(int n) { return 2048 / diag_tile_w(n) < n ? 2048 / diag_tile_w(n) : n; }
+__host__ __device__ constexpr int diag_tiles(int n) { return (n / diag_tile_w(n)) * (n / diag_tile_h(n)); }
+__host__ __device__ constexpr int diag_zonal_ctas(int n) { return (n + 7) / 8; }
 __host__ __device__ constexpr size_t diag_all_smem(int n) {
   return (sizeof(double) + sizeof(uint32_t)) * (size_t)(n / 2 + 3);
 }
-__global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, double* out, uint32_t* bins, int n) {
+__global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, const float2* __restrict__ vel,
+                                                  double* out, uint32_t* bins, float* zonal, int n) {
+  const int tiles = diag_tiles(n);
+  if ((int)blockIdx.x >= tiles) {   // zonal mean of u, FP64 accumulation
+    const int row = ((int)blockIdx.x - tiles) * 8 + (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float4* r4 = reinterpret_cast<const float4*>(vel + (size_t)row * n);
+    double acc = 0.0;
+    for (int i = lane; i < n / 2; i += 32) {
+      const float4 t = r4[i];
+      acc += (double)t.x;
+      acc += (double)t.z;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) zonal[row] = (float)(acc / n);
+    return;
+  }
   extern __shared__ double hist[];
   const int nb = n / 2 + 1;
   uint32_t* fhist = reinterpret_cast<uint32_t*>(hist + nb + 2);
@@ -234,14 +263,16 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
     fhist[i] = 0u;
   }
   __syncthreads();
-  const double n4 = (double)n * n * (double)n * n;
-  const float n2f = (float)n * (float)n;
+  const int tw = diag_tile_w(n), th = diag_tile_h(n), per_row = tw / kDiagCells;
+  const int tiles_x = n / tw;
+  const double inv_n4 = 1.0 / ((double)n * n * (double)n * n);
+  const float inv_n4f = 1.f / ((float)n * (float)n * ((float)n * (float)n));
   const float kcut = (float)(n / 3.0);
-  const int per_row = n / kDiagCells;
   double ene = 0.0, ens = 0.0;
   uint32_t fe = 0u, fz = 0u;
-  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n * per_row; it += gridDim.x * blockDim.x) {
-    const int row = it / per_row, c0 = (it - row * per_row) * kDiagCells;
+  if ((int)threadIdx.x < th * per_row) {
+    const int row = ((int)blockIdx.x / tiles_x) * th + (int)threadIdx.x / per_row;
+    const int c0 = ((int)blockIdx.x % tiles_x) * tw + ((int)threadIdx.x % per_row) * kDiagCells;
     const int ky = row < n / 2 ? row : row - n;
     const float kyf = (float)ky;
     const float4* p = reinterpret_cast<const float4*>(w + (size_t)row * n + c0);
@@ -260,14 +291,19 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
       const int col = c0 + j;
       const int kx = col < n / 2 ? col : col - n;
       const float2 a = v[j];
+      const int k2i = kx * kx + ky * ky;
+      const float kxf = (float)kx;
+      const float k2f = kxf * kxf + kyf * kyf;                       // exact (k2 < 2^24)
+      const int fb_raw = (int)(sqrtf(k2f) + 0.5f);
       // FP64
-      const double k2 = (double)kx * kx + (double)ky * ky;
-      const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) / n4;
+      const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) * inv_n4;
       ens += z;
-      if (k2 > 0.0) {
-        const double e = z / k2;
+      if (k2i > 0) {
+        const double e = z / (double)k2i;
         ene += e;
-        int b = (int)floor(sqrt(k2) + 0.5);
+        int b = fb_raw;
+        if (b * b - b >= k2i) --b;
+        else if (b * b + b < k2i) ++b;
         b = b < nb - 1 ? b : nb - 1;
         if (b != cur_b) {
           if (cur_b >= 0) atomicAdd(&hist[cur_b], cur_e);
@@ -277,12 +313,10 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
         cur_e += e;
       }
       // u32 fixed point
-      const float kxf = (float)kx;
-      const float k2f = kxf * kxf + kyf * kyf;
       if (k2f != 0.f && fabsf(kxf) < kcut && fabsf(kyf) < kcut) {
-        const float ensf = 0.5f * (a.x * a.x + a.y * a.y) / (n2f * n2f);
+        const float ensf = 0.5f * (a.x * a.x + a.y * a.y) * inv_n4f;
         const float enef = ensf / k2f;
-        const int fb = (int)min((uint32_t)(sqrtf(k2f) + 0.5f), (uint32_t)(nb - 1));
+        const int fb = (int)min((uint32_t)fb_raw, (uint32_t)(nb - 1));
         if (fb != cur_fb) {
           if (cur_fb >= 0) atomicAdd(&fhist[cur_fb], cur_f);
           cur_fb = fb;
@@ -313,22 +347,6 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
   for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) {
     if (hist[i] != 0.0) atomicAdd(&out[i], hist[i]);
     if (fhist[i] != 0u) atomicAdd(&bins[i], fhist[i]);
-  }
-}
-
-// zonal mean of u per row (spectrum.wgsl:41-68), accumulated in FP64
-__global__ void k_zonal_mean(const float2* __restrict__ vel, float* zonal, int n) {
-  const int row = blockIdx.x;
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += (double)vel[(size_t)row * n + i].x;
-  acc = warp_sum(acc);
-  __shared__ double red[32];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < (int)blockDim.x / 32; ++i) s += red[i];
-    zonal[row] = (float)(s / n);
   }
 }
 
