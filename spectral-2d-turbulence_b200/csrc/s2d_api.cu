@@ -479,8 +479,11 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMallocHost(&s->h_upload, kUploadSlotBytes * kUploadSlots), "pinned upload ring");
   for (cudaEvent_t& ev : s->upload_ev) TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
   TRY(set_all_attrs(*ops), "kernel attributes");
-  TRY(cudaFuncSetAttribute(k_dye_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)dye_fused_smem(n, s->m)), "dye kernel attributes");
+  if (dye_wide_tile(n, s->m))
+    TRY(cudaFuncSetAttribute(k_dye_fused<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)DyeGeom<64>::smem(n, s->m)), "dye kernel attributes");
+  TRY(cudaFuncSetAttribute(k_dye_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)DyeGeom<32>::smem(n, s->m)), "dye kernel attributes");
   if (fft_precision == S2D_FFT_TC_F16) TRY(tc_attrs<tc::PrecF16>(), "tensor-core kernel attributes");
   if (fft_precision == S2D_FFT_TC_BF16) TRY(tc_attrs<tc::PrecBF16>(), "tensor-core kernel attributes");
   // zero everything the reference's fresh buffers hold as zero
@@ -781,10 +784,16 @@ extern "C" int s2d_encode_dye(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
   const int p = s->dye_parity, m = s->m;
-  const dim3 grd((m + kDyeTile - 1) / kDyeTile, (m + kDyeTile - 1) / kDyeTile);
   ProfScope ps(s, S2D_PROF_DYE);
-  k_dye_fused<<<grd, kDyeThreads, dye_fused_smem(s->n, m), s->stream>>>(
-      s->vel, tex(s, p), tex(s, 1 - p), dt_slot(s, s->slot), s->dparams, s->dsplats, s->n, m);
+  if (dye_wide_tile(s->n, m)) {
+    using G = DyeGeom<64>;
+    k_dye_fused<64><<<dim3(m / 64, m / G::TY), G::THREADS, G::smem(s->n, m), s->stream>>>(
+        s->vel, tex(s, p), tex(s, 1 - p), dt_slot(s, s->slot), s->dparams, s->dsplats, s->n, m);
+  } else {
+    using G = DyeGeom<32>;
+    k_dye_fused<32><<<dim3(m / 32, m / G::TY), G::THREADS, G::smem(s->n, m), s->stream>>>(
+        s->vel, tex(s, p), tex(s, 1 - p), dt_slot(s, s->slot), s->dparams, s->dsplats, s->n, m);
+  }
   S2D_LAUNCHED();
   s->dye_parity = 1 - p;
   return S2D_OK;

@@ -8,18 +8,18 @@
 // Two implementations share every sampling function, so they agree bit for bit:
 //   * three passes (advect_fwd, advect_back, advect_corr) exactly as the
 //     reference dispatches them, each reading and writing whole textures;
-//   * k_dye_fused: one launch per step.  A CTA owns a 32 x 32 output tile and
-//     keeps, in shared memory, the source texels of the tile plus a 3-level halo,
-//     the forward-pass texels of the tile plus 2 levels and the backward-pass
-//     texels plus 1 level; each level's halo (1 texel below, 2 above) covers the
-//     bilinear footprint of a back-trace of up to one texel, which the CFL limit
-//     gives at dyeScale 2.  A sample outside the on-chip region is recomputed from global
-//     memory (the forward/backward values at that texel are re-derived), so the
-//     result does not depend on the halo being large enough.  Texture traffic
-//     drops from 7 texture passes to one read and one write.  The forward and
-//     backward windows hold the binary16 values those textures would hold
-//     (exact), the source window their FP32 expansion, and only r, g, b are
-//     carried: the corrected texel's alpha is 1 whatever the inputs.
+//   * k_dye_fused: one launch per step.  A CTA owns a TX x 32 output tile (TX = 64,
+//     or 32 when the dye is not refined over the flow) and keeps, in shared memory,
+//     the source texels of the tile plus a 3-level halo, the forward-pass texels of
+//     the tile plus 2 levels and the backward-pass texels plus 1 level; each level's
+//     halo (1 texel below, 2 above) covers the bilinear footprint of a back-trace of
+//     up to one texel, which the CFL limit gives at dyeScale 2.  A sample outside the
+//     on-chip region is recomputed from global memory (the forward/backward values at
+//     that texel are re-derived), so the result does not depend on the halo being
+//     large enough.  Texture traffic drops from 7 texture passes to one read and one
+//     write.  The source, forward and backward windows hold binary16 texels, as those
+//     textures would (exact), and only r, g, b are carried: the corrected texel's
+//     alpha is 1 whatever the inputs.
 #pragma once
 #include <cuda_fp16.h>
 #include "s2d_device.cuh"
@@ -54,7 +54,9 @@ struct GlobalVel {
 };
 
 // Every operation below is an explicitly rounded intrinsic (no multiply-add
-// contraction), so the fused and the three-pass kernels produce the same bits.
+// contraction), so the fused and the three-pass kernels produce the same bits.  Where a
+// product is exact -- a coordinate in [0, 1] times the power-of-two grid size -- the
+// multiply and the following add are one fused multiply-add with the same result.
 __device__ __forceinline__ float lerp1(float a, float b, float t) {
   return __fmaf_rn(b, t, __fmul_rn(a, __fsub_rn(1.f, t)));   // WGSL mix(a, b, t)
 }
@@ -63,7 +65,7 @@ __device__ __forceinline__ float lerp1(float a, float b, float t) {
 template <class VF>
 __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, int n) {
   const float nf = (float)n;
-  const float gx = __fsub_rn(__fmul_rn(px, nf), 0.5f), gy = __fsub_rn(__fmul_rn(py, nf), 0.5f);
+  const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
   const float bx = floorf(gx), by = floorf(gy);
   const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
   const int ix = (int)bx, iy = (int)by;
@@ -79,10 +81,12 @@ __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - 
 }
 
 // midpoint back-trace (dye.wgsl:40-45), from the velocity v1 already sampled at p
+// (0.5 (v h) is v (h/2): halving commutes with the rounding of the product)
 template <class VF>
 __device__ __forceinline__ float2 trace_from(const VF& vf, float px, float py, float2 v1, float h, int n) {
-  const float mx = fract_shift(px, __fmul_rn(0.5f, __fmul_rn(v1.x, h)));
-  const float my = fract_shift(py, __fmul_rn(0.5f, __fmul_rn(v1.y, h)));
+  const float hh = 0.5f * h;
+  const float mx = fract_shift(px, __fmul_rn(v1.x, hh));
+  const float my = fract_shift(py, __fmul_rn(v1.y, hh));
   const float2 v2 = sample_vel(vf, mx, my, n);
   return make_float2(fract_shift(px, __fmul_rn(v2.x, h)), fract_shift(py, __fmul_rn(v2.y, h)));
 }
@@ -98,7 +102,7 @@ struct Footprint {
 };
 __device__ __forceinline__ Footprint footprint(float sx, float sy, int m) {
   const float mf = (float)m;
-  const float gx = __fsub_rn(__fmul_rn(sx, mf), 0.5f), gy = __fsub_rn(__fmul_rn(sy, mf), 0.5f);
+  const float gx = __fmaf_rn(sx, mf, -0.5f), gy = __fmaf_rn(sy, mf, -0.5f);   // sx * mf exact
   const float bx = floorf(gx), by = floorf(gy);
   Footprint f;
   f.fx = __fsub_rn(gx, bx);
@@ -129,11 +133,12 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
           lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
 }
 
-// texel centre (x + 0.5)/m; m is a power of two, so the product with 1/m is the
-// exactly rounded quotient
+// texel centre (x + 0.5)/m; m is a power of two, so x/m, 0.5/m and their sum (2x+1)/(2m)
+// are all exact and one fused multiply-add gives the quotient
 __device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
   const float inv = __frcp_rn((float)m);
-  return make_float2(__fmul_rn(__fadd_rn((float)x, 0.5f), inv), __fmul_rn(__fadd_rn((float)y, 0.5f), inv));
+  const float half_inv = 0.5f * inv;
+  return make_float2(__fmaf_rn((float)x, inv, half_inv), __fmaf_rn((float)y, inv, half_inv));
 }
 
 // BFECC correction of one texel from its source (a, with the 4-texel min/max) and
@@ -198,24 +203,36 @@ __global__ void k_dye_correct(const float2* __restrict__ vel, const uint2* __res
 }
 
 // ---------------------------------------------------------------- fused single pass
-constexpr int kDyeTile = 32;         // output tile edge
 // Halo per level: a sample displaced by at most one texel from texel x has the bilinear
 // footprint [x - 1, x + 2], so each level extends the region below by 1 and above by 2.
 constexpr int kDyeLo = 1, kDyeHi = 2;
-constexpr int kDyeThreads = 256;
-constexpr int kDyeW1 = kDyeTile + (kDyeLo + kDyeHi);       // backward-pass region edge
-constexpr int kDyeW2 = kDyeTile + 2 * (kDyeLo + kDyeHi);   // forward-pass region edge
-constexpr int kDyeW3 = kDyeTile + 3 * (kDyeLo + kDyeHi);   // source region edge
-
-// velocity cells needed by traces from the forward-pass region, for an n x n velocity grid
-// under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation/rounding cells
-__host__ __device__ constexpr int dye_vel_edge(int n, int m) { return (kDyeW2 + 2) * n / m + 4; }
-// binary16 source / forward / backward windows; FP32 centre velocities and forward trace
-// positions of the forward region; the velocity window
-__host__ __device__ constexpr size_t dye_fused_smem(int n, int m) {
-  return sizeof(uint2) * (kDyeW3 * kDyeW3 + kDyeW1 * kDyeW1 + kDyeW2 * kDyeW2) +
-         sizeof(float2) * (2 * kDyeW2 * kDyeW2 + dye_vel_edge(n, m) * dye_vel_edge(n, m));
-}
+constexpr int kDyeTileY = 32;
+// Output tile TX x 32 (TX = 64 when the dye is refined over the flow: 112 KB of windows,
+// 2 CTAs of 512 threads per SM, and 30 % / 15 % of recomputed forward / backward halo
+// texels instead of 41 % / 20 % at TX = 32; TX = 32 otherwise, where the velocity window
+// is as large as the dye windows)
+template <int TX> struct DyeGeom {
+  static constexpr int TY = kDyeTileY;
+  static constexpr int THREADS = TX * 8;
+  static constexpr int MINB = TX >= 64 ? 2 : 3;   // resident CTAs per SM (shared memory bound)
+  static constexpr int H = kDyeLo + kDyeHi;
+  static constexpr int W1X = TX + H, W1Y = TY + H;           // backward-pass region
+  static constexpr int W2X = TX + 2 * H, W2Y = TY + 2 * H;   // forward-pass region
+  static constexpr int W3X = TX + 3 * H, W3Y = TY + 3 * H;   // source region
+  // velocity cells needed by traces from the forward-pass region, for an n x n velocity
+  // grid under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation /
+  // rounding cells on each side
+  __host__ __device__ static constexpr int vel_x(int n, int m) { return (W2X + 2) * n / m + 4; }
+  __host__ __device__ static constexpr int vel_y(int n, int m) { return (W2Y + 2) * n / m + 4; }
+  // binary16 source / backward / forward windows; FP32 centre velocities and forward
+  // trace positions of the forward region; the velocity window
+  __host__ __device__ static constexpr size_t smem(int n, int m) {
+    return sizeof(uint2) * (W3X * W3Y + W1X * W1Y + W2X * W2Y) +
+           sizeof(float2) * (2 * W2X * W2Y + vel_x(n, m) * vel_y(n, m));
+  }
+};
+// the wide tile for dye grids at least 2x the velocity grid and 64 texels wide
+inline bool dye_wide_tile(int n, int m) { return m >= 64 && m >= 2 * n; }
 
 // 8-byte asynchronous global -> shared copy (no register staging) and its wait
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -236,21 +253,23 @@ __device__ __forceinline__ Rgb rgb_of(uint2 u) {
 // binary16 texel (r, g, b, alpha 1) of FP32 channels, as a texture store rounds them
 __device__ __forceinline__ uint2 pack_rgb(const Rgb& c) { return pack_texel(c.r, c.g, c.b, 1.f); }
 
-// on-chip window of binary16 source texels with an exact global fallback (coordinates
-// are wrapped indices)
+// on-chip W x WY window of binary16 source texels with an exact global fallback
+// (coordinates are wrapped indices)
+template <int W, int WY>
 struct SmemTex {
+  static constexpr int w = W, wy = WY;
   const uint2* sm;
-  int ox, oy, w, m;
+  int ox, oy, m;   // window origin (wrapped), dye grid size
   const uint2* g;
   __device__ __forceinline__ Rgb operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return rgb_of(sm[ry * w + rx]);
+    if (rx < w && ry < wy) return rgb_of(sm[ry * w + rx]);
     return rgb_of(__ldg(g + (size_t)y * m + x));
   }
   // the 2x2 footprint in one window test (slots rx, rx+1 hold texels x0, x1 = x0+1 wrapped)
   __device__ __forceinline__ bool quad(const Footprint& f, Rgb (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
-    if (rx + 1 < w && ry + 1 < w) {
+    if (rx + 1 < w && ry + 1 < wy) {
       const uint2* p = sm + ry * w + rx;
       c[0] = rgb_of(p[0]);
       c[1] = rgb_of(p[1]);
@@ -263,11 +282,11 @@ struct SmemTex {
 };
 struct SmemVel {
   const float2* sm;
-  int ox, oy, w, n;
+  int ox, oy, w, wy, n;   // window origin, row length (x extent), y extent
   const float2* g;
   __device__ __forceinline__ float2 operator()(int x, int y) const {
     const int rx = (x - ox) & (n - 1), ry = (y - oy) & (n - 1);
-    if (rx < w && ry < w) return sm[ry * w + rx];
+    if (rx < w && ry < wy) return sm[ry * w + rx];
     return __ldg(g + (size_t)y * n + x);
   }
 };
@@ -276,13 +295,13 @@ struct SmemVel {
 __device__ __forceinline__ float2 sample_vel_win(const SmemVel& vf, float px, float py) {
   const int n = vf.n;
   const float nf = (float)n;
-  const float gx = __fsub_rn(__fmul_rn(px, nf), 0.5f), gy = __fsub_rn(__fmul_rn(py, nf), 0.5f);
+  const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
   const float bx = floorf(gx), by = floorf(gy);
   const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
   const int ix = (int)bx, iy = (int)by;
   const int rx = (ix - vf.ox) & (n - 1), ry = (iy - vf.oy) & (n - 1);
   float2 v00, v10, v01, v11;
-  if (rx + 1 < vf.w && ry + 1 < vf.w) {
+  if (rx + 1 < vf.w && ry + 1 < vf.wy) {
     const float2* p = vf.sm + ry * vf.w + rx;
     v00 = p[0];
     v10 = p[1];
@@ -329,20 +348,21 @@ __device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb*
           lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy)};
 }
 
-// binary16 window whose texels outside the window are re-derived by EVAL
-template <class EVAL>
+// binary16 W x WY window whose texels outside the window are re-derived by EVAL
+template <class EVAL, int W, int WY>
 struct DerivedTex {
+  static constexpr int w = W, wy = WY;
   const uint2* sm;
-  int ox, oy, w, m;
+  int ox, oy, m;   // window origin (wrapped), dye grid size
   const EVAL& eval;
   __device__ __forceinline__ Rgb operator()(int x, int y) const {
     const int rx = (x - ox) & (m - 1), ry = (y - oy) & (m - 1);
-    if (rx < w && ry < w) return rgb_of(sm[ry * w + rx]);
+    if (rx < w && ry < wy) return rgb_of(sm[ry * w + rx]);
     return rgb_of(eval(x, y));
   }
   __device__ __forceinline__ bool quad(const Footprint& f, Rgb (&c)[4]) const {
     const int rx = (f.x0 - ox) & (m - 1), ry = (f.y0 - oy) & (m - 1);
-    if (rx + 1 < w && ry + 1 < w) {
+    if (rx + 1 < w && ry + 1 < wy) {
       const uint2* p = sm + ry * w + rx;
       c[0] = rgb_of(p[0]);
       c[1] = rgb_of(p[1]);
@@ -355,9 +375,10 @@ struct DerivedTex {
 };
 
 // forward-pass texel (x, y) as the advect_fwd texture would hold it
+template <class TS>
 struct FwdEval {
   const SmemVel& vel;
-  const SmemTex& src;
+  const TS& src;
   float h;
   int n, m;
   __device__ __forceinline__ uint2 operator()(int x, int y) const {
@@ -366,11 +387,11 @@ struct FwdEval {
     return pack_rgb(bilerp_rgb(src, footprint(s.x, s.y, m)));
   }
 };
-using FwdFetch = DerivedTex<FwdEval>;
 // backward-pass texel (x, y) as the advect_back texture would hold it
+template <class FF>
 struct BackEval {
   const SmemVel& vel;
-  const FwdFetch& fwd;
+  const FF& fwd;
   float h;
   int n, m;
   __device__ __forceinline__ uint2 operator()(int x, int y) const {
@@ -379,7 +400,6 @@ struct BackEval {
     return pack_rgb(bilerp_rgb(fwd, footprint(s.x, s.y, m)));
   }
 };
-using BackFetch = DerivedTex<BackEval>;
 
 // BFECC correction from r, g, b (the arithmetic of correct_from; alpha is not read)
 __device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const Rgb& lo, const Rgb& hi, float px,
@@ -388,19 +408,23 @@ __device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const R
   return correct_from(a4, b4, lo4, hi4, px, py, fade, S);
 }
 
-__global__ void __launch_bounds__(kDyeThreads)
+template <int TX>
+__global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
                 const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
                 const DevSplats* __restrict__ S, int n, int m) {
+  using G = DyeGeom<TX>;
+  constexpr int TY = G::TY, NT = G::THREADS;
+  constexpr int W1X = G::W1X, W1Y = G::W1Y, W2X = G::W2X, W2Y = G::W2Y, W3X = G::W3X, W3Y = G::W3Y;
   extern __shared__ uint2 dsm2[];
   uint2* s_src = dsm2;
-  uint2* s_back = s_src + kDyeW3 * kDyeW3;
-  uint2* s_fwd = s_back + kDyeW1 * kDyeW1;
-  float2* s_v1 = reinterpret_cast<float2*>(s_fwd + kDyeW2 * kDyeW2);   // velocity at forward-region texels
-  float2* s_sp = s_v1 + kDyeW2 * kDyeW2;                                // their forward trace positions
-  float2* s_vel = s_sp + kDyeW2 * kDyeW2;
-  const int vw = dye_vel_edge(n, m);
-  const int tx0 = blockIdx.x * kDyeTile, ty0 = blockIdx.y * kDyeTile;
+  uint2* s_back = s_src + W3X * W3Y;
+  uint2* s_fwd = s_back + W1X * W1Y;
+  float2* s_v1 = reinterpret_cast<float2*>(s_fwd + W2X * W2Y);   // velocity at forward-region texels
+  float2* s_sp = s_v1 + W2X * W2Y;                                // their forward trace positions
+  float2* s_vel = s_sp + W2X * W2Y;
+  const int vwx = G::vel_x(n, m), vwy = G::vel_y(n, m);
+  const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
   const float h = __fdiv_rn(dtbuf[0], kTwoPiF);
 
@@ -414,24 +438,25 @@ __global__ void __launch_bounds__(kDyeThreads)
 
   // the source window arrives asynchronously while the traces below (velocity only) run
 #pragma unroll 4
-  for (int i = tid; i < kDyeW3 * kDyeW3; i += kDyeThreads) {
-    const int ry = i / kDyeW3, rx = i - ry * kDyeW3;
+  for (int i = tid; i < W3X * W3Y; i += NT) {
+    const int ry = i / W3X, rx = i - ry * W3X;
     cp_async8(s_src + i, src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
   }
   cp_async_commit();
 #pragma unroll 4
-  for (int i = tid; i < vw * vw; i += kDyeThreads) {
-    const int ry = i / vw, rx = i - ry * vw;
+  for (int i = tid; i < vwx * vwy; i += NT) {
+    const int ry = i / vwx, rx = i - ry * vwx;
     s_vel[i] = __ldg(vel + (size_t)((vyw + ry) & (n - 1)) * n + ((vxw + rx) & (n - 1)));
   }
   __syncthreads();
 
-  const SmemVel V{s_vel, vxw, vyw, vw, n, vel};
-  const SmemTex T{s_src, sx0, sy0, kDyeW3, m, src};
+  const SmemVel V{s_vel, vxw, vyw, vwx, vwy, n, vel};
+  using Tex = SmemTex<W3X, W3Y>;
+  const Tex T{s_src, sx0, sy0, m, src};
   // velocity at every forward-region texel centre (shared by the +h and -h traces) and
   // the forward trace from it
-  for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
-    const int ry = i / kDyeW2, rx = i - ry * kDyeW2;
+  for (int i = tid; i < W2X * W2Y; i += NT) {
+    const int ry = i / W2X, rx = i - ry * W2X;
     const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
     const float2 v1 = sample_vel_win(V, p.x, p.y);
     s_v1[i] = v1;
@@ -441,32 +466,35 @@ __global__ void __launch_bounds__(kDyeThreads)
   __syncthreads();
 
   // forward pass over the forward region
-  for (int i = tid; i < kDyeW2 * kDyeW2; i += kDyeThreads) {
+  for (int i = tid; i < W2X * W2Y; i += NT) {
     const float2 sp = s_sp[i];
     s_fwd[i] = pack_rgb(bilerp_rgb(T, footprint(sp.x, sp.y, m)));
   }
   __syncthreads();
 
-  const FwdEval fe{V, T, h, n, m};
-  const FwdFetch ff{s_fwd, fx0, fy0, kDyeW2, m, fe};
+  using FE = FwdEval<Tex>;
+  using FF = DerivedTex<FE, W2X, W2Y>;
+  const FE fe{V, T, h, n, m};
+  const FF ff{s_fwd, fx0, fy0, m, fe};
   // backward pass over the backward region (nested in the forward region by kDyeLo / kDyeHi)
-  for (int i = tid; i < kDyeW1 * kDyeW1; i += kDyeThreads) {
-    const int ry = i / kDyeW1, rx = i - ry * kDyeW1;
-    const int fi = (ry + kDyeLo) * kDyeW2 + rx + kDyeLo;
+  for (int i = tid; i < W1X * W1Y; i += NT) {
+    const int ry = i / W1X, rx = i - ry * W1X;
+    const int fi = (ry + kDyeLo) * W2X + rx + kDyeLo;
     const float2 p = texel_pos((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1), m);
     const float2 sb = trace_from(WinVel{V}, p.x, p.y, s_v1[fi], -h, n);
     s_back[i] = pack_rgb(bilerp_rgb(ff, footprint(sb.x, sb.y, m)));
   }
   __syncthreads();
 
-  const BackEval be{V, ff, h, n, m};
-  const BackFetch bf{s_back, bx0, by0, kDyeW1, m, be};
+  using BE = BackEval<FF>;
+  const BE be{V, ff, h, n, m};
+  const DerivedTex<BE, W1X, W1Y> bf{s_back, bx0, by0, m, be};
   const float fade = params->dye_fade;
-  for (int i = tid; i < kDyeTile * kDyeTile; i += kDyeThreads) {
-    const int ry = i / kDyeTile, rx = i - ry * kDyeTile;
+  for (int i = tid; i < TX * TY; i += NT) {
+    const int ry = i / TX, rx = i - ry * TX;
     const int x = tx0 + rx, y = ty0 + ry;
     const float2 p = texel_pos(x, y, m);
-    const float2 sp = s_sp[(ry + 2 * kDyeLo) * kDyeW2 + rx + 2 * kDyeLo];
+    const float2 sp = s_sp[(ry + 2 * kDyeLo) * W2X + rx + 2 * kDyeLo];
     const Footprint f = footprint(sp.x, sp.y, m);
     Rgb lo, hi;
     const Rgb a = bilerp_rgb(T, f, &lo, &hi);

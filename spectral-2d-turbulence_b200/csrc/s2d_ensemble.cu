@@ -62,15 +62,15 @@ constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
 constexpr size_t kEnsASmem =
     cmax(cmax(cmax(Tune<64>::A_SMEM, Tune<128>::A_SMEM), cmax(Tune<256>::A_SMEM, Tune<512>::A_SMEM)),
          Tune<1024>::A_SMEM);
-// one layout for every size: exchange lines, staged rows, then the barrier
-constexpr size_t kEnsBStageOff =
+// one layout for every size: exchange lines, then the tile barrier (the default shapes
+// stage no rows)
+static_assert(!Tune<64>::PREFETCH && !Tune<128>::PREFETCH && !Tune<256>::PREFETCH && !Tune<512>::PREFETCH &&
+                  !Tune<1024>::PREFETCH,
+              "ensemble row tiles use no staging");
+constexpr size_t kEnsBBarOff =
     cmax(cmax(cmax(Tune<64>::B_SMEM, Tune<128>::B_SMEM), cmax(Tune<256>::B_SMEM, Tune<512>::B_SMEM)),
          Tune<1024>::B_SMEM);
-constexpr size_t kEnsBStageBytes =
-    cmax(cmax(cmax(Tune<64>::B_STAGE_BYTES, Tune<128>::B_STAGE_BYTES),
-              cmax(Tune<256>::B_STAGE_BYTES, Tune<512>::B_STAGE_BYTES)),
-         Tune<1024>::B_STAGE_BYTES);
-constexpr size_t kEnsBSmem = kEnsBStageOff + kEnsBStageBytes + 16;
+constexpr size_t kEnsBSmem = kEnsBBarOff + 16;
 
 struct Pools {
   float2* s[3];
@@ -102,13 +102,6 @@ __global__ void __launch_bounds__(kEnsAThreads, MINB)
   }
 }
 
-// the per-size tile functions place staged rows and the barrier at Tune<N> offsets;
-// the ensemble kernel hands each size a window whose offsets match by shifting the
-// base pointer so that Tune<N>::B_STAGE_OFF lands on the common staging offset
-template <int N> __device__ __forceinline__ float2* ens_spec_base(float2* smem) {
-  return reinterpret_cast<float2*>(reinterpret_cast<char*>(smem) + (kEnsBStageOff - Tune<N>::B_STAGE_OFF));
-}
-
 // MINB: resident CTAs per SM the register allocation must allow.  Over pooled state far
 // larger than L2 the row pass waits on HBM, and more CTAs in flight hide more of it even
 // with some registers spilled to L1 (256 x 256^2: 761 -> 831 ensemble-steps/s going from
@@ -119,7 +112,7 @@ __global__ void __launch_bounds__(kEnsBThreads, MINB)
                int* err) {
   extern __shared__ __align__(16) float2 smem[];
   const int st = MODE < 0 ? 0 : MODE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + kEnsBStageOff + kEnsBStageBytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(smem) + kEnsBBarOff);
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
@@ -142,11 +135,11 @@ __global__ void __launch_bounds__(kEnsBThreads, MINB)
     a.stochastic = I.p.force_amp > 0.f ? 1 : 0;
     a.err = err;
     switch (I.n) {
-      case 64: spec_rows_tile<64, MODE, false>(a, it.y, ens_spec_base<64>(smem), bar, parity); break;
-      case 128: spec_rows_tile<128, MODE, false>(a, it.y, ens_spec_base<128>(smem), bar, parity); break;
-      case 256: spec_rows_tile<256, MODE, false>(a, it.y, ens_spec_base<256>(smem), bar, parity); break;
-      case 512: spec_rows_tile<512, MODE, false>(a, it.y, ens_spec_base<512>(smem), bar, parity); break;
-      default: spec_rows_tile<1024, MODE, false>(a, it.y, ens_spec_base<1024>(smem), bar, parity); break;
+      case 64: spec_rows_tile<64, MODE, false>(a, it.y, smem, bar, parity); break;
+      case 128: spec_rows_tile<128, MODE, false>(a, it.y, smem, bar, parity); break;
+      case 256: spec_rows_tile<256, MODE, false>(a, it.y, smem, bar, parity); break;
+      case 512: spec_rows_tile<512, MODE, false>(a, it.y, smem, bar, parity); break;
+      default: spec_rows_tile<1024, MODE, false>(a, it.y, smem, bar, parity); break;
     }
     __syncthreads();
   }

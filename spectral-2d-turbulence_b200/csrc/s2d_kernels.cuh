@@ -27,10 +27,11 @@ namespace s2d {
 
 // Launch shape of the stage kernels for N x N: V values per thread (T = N/V threads per
 // line; the line FFT runs radix-V passes), GA columns per column-kernel CTA, PPB row pairs
-// per row-kernel CTA, and the resident CTAs the register budget must allow (AMB_/BMB_;
-// 0 = as many as 128 registers a thread give).  Tune<N> is the default shape; the
+// per row-kernel CTA, the resident CTAs the register budget must allow (AMB_/BMB_;
+// 0 = as many as 128 registers a thread give), and whether the row kernel stages the
+// rows its RK update reads by bulk copy (PF_).  Tune<N> is the default shape; the
 // autotuner picks among the variants each size registers (s2d_ops.cuh).
-template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0> struct Tune {
+template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0, bool PF_ = false> struct Tune {
   static constexpr int N = N_;
   static constexpr int V = V_;
   static constexpr int T = N / V;
@@ -52,15 +53,15 @@ template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0> struct Tune {
   static constexpr int B_MINB = BMB_ ? BMB_ : (65536 / (B_THREADS * 128) > 0 ? 65536 / (B_THREADS * 128) : 1);
   static constexpr size_t A_SMEM = sizeof(float2) * 2 * GA * A_LDS;
   static constexpr size_t B_SMEM = sizeof(float2) * 2 * B_ROWS * B_LDS;
-  // rows the spectral-row kernel can stage by TMA bulk copy (wcur, w0, pointer force)
-  // after the exchange lines.  Off: measured at 1024^2 the 48 KB of staging halves the
-  // resident CTAs (4 -> 2 per SM) and the kernel slows from 30 to 40 us, more than the
-  // overlap with the x-FFT of Z recovers.
-  static constexpr bool PREFETCH = false;
-  static constexpr size_t B_STAGE_OFF = B_SMEM;
-  static constexpr size_t B_STAGE_BYTES = PREFETCH ? sizeof(float2) * 3 * B_ROWS * N : 0;
-  static constexpr size_t B_BAR_OFF = B_STAGE_OFF + B_STAGE_BYTES;
-  static constexpr size_t B_SMEM_TOTAL = B_BAR_OFF + 16;
+  // PF_: the spectral-row kernel stages the rows its RK update reads (wcur, w0 from
+  // stage 1 on, the pointer force when splats are active) by bulk copy into shared
+  // memory after the exchange lines; they land while the Z loads and the x-FFT run.  The
+  // staging is sized per kernel instance (spec_smem): 16 KB a row pair per array at
+  // 1024^2, so the stage kernels without pointer forcing keep 3 CTAs per SM.
+  static constexpr bool PREFETCH = PF_;
+  static constexpr size_t B_BAR_OFF = B_SMEM;
+  static constexpr size_t B_STAGE_OFF = B_SMEM + 16;
+  static constexpr size_t B_SMEM_TOTAL = B_STAGE_OFF;   // without staging
   static constexpr size_t COLS_SMEM = sizeof(float2) * GA * A_LDS;
   static constexpr size_t ROWS_SMEM = sizeof(float2) * B_ROWS * B_LDS;
 };
@@ -126,6 +127,12 @@ template <int N, class TU = Tune<N>> __device__ __forceinline__ int spec_row_of(
 // number of staged row arrays for a stage: wcur, w0 (stages 1-2), pointer force
 template <int MODE, bool PTR> __host__ __device__ constexpr int spec_stage_arrays() {
   return (MODE >= 1 ? 2 : 1) + (PTR ? 1 : 0);
+}
+// dynamic shared memory of one spectral-row kernel instance: exchange lines, tile
+// barrier, then (PF_) the staged rows
+template <class TU, int MODE, bool PTR> __host__ __device__ constexpr size_t spec_smem() {
+  return TU::B_STAGE_OFF +
+         (TU::PREFETCH ? sizeof(float2) * spec_stage_arrays<MODE, PTR>() * TU::B_ROWS * TU::N : 0);
 }
 
 // ---------------------------------------------------------------------------------------

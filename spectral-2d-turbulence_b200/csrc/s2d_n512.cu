@@ -7,7 +7,8 @@ const NOps* ops_n512() {
   // extra stage shapes the autotuner may pick (radix-8 line passes, more resident CTAs)
   static const NOps o = OpsImpl<512>::make({PhysImpl<512, Tune<512, 8>>::make("V=8")},
                                       {SpecImpl<512, Tune<512, 8>>::make("V=8"),
-                                       SpecImpl<512, Tune<512, 8, 0, 6>>::make("V=8, 6 CTAs/SM")});
+                                       SpecImpl<512, Tune<512, 8, 0, 6>>::make("V=8, 6 CTAs/SM"),
+                                       SpecImpl<512, Tune<512, 8, 0, 6, true>>::make("V=8, 6 CTAs/SM, staged rows")});
   return &o;
 }
 }  // namespace s2d

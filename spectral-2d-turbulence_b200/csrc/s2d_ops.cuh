@@ -61,34 +61,30 @@ template <int N, class TU> struct PhysImpl {
 
 // ---------------------------------------------------------------- row-stage variant
 template <int N, class TU> struct SpecImpl {
+  template <int MODE, bool PTR> static cudaError_t attr() {
+    return set_smem(k_spec_rows<N, MODE, PTR, TU>, spec_smem<TU, MODE, PTR>());
+  }
   static cudaError_t set_attrs() {
     cudaError_t e = cudaSuccess;
     auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
-    chk(set_smem(k_spec_rows<N, -1, false, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 0, false, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 1, false, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 2, false, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 0, true, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 1, true, TU>, TU::B_SMEM_TOTAL));
-    chk(set_smem(k_spec_rows<N, 2, true, TU>, TU::B_SMEM_TOTAL));
+    chk(attr<-1, false>());
+    chk(attr<0, false>());
+    chk(attr<1, false>());
+    chk(attr<2, false>());
+    chk(attr<0, true>());
+    chk(attr<1, true>());
+    chk(attr<2, true>());
     return e;
   }
+  template <int MODE, bool PTR> static void launch(const SpecArgs& a, cudaStream_t st) {
+    k_spec_rows<N, MODE, PTR, TU><<<dim3(TU::B_GRID), dim3(TU::B_THREADS), spec_smem<TU, MODE, PTR>(), st>>>(a);
+  }
   static void run(int mode, bool ptr, const SpecArgs& a, cudaStream_t st) {
-    const dim3 g(TU::B_GRID), b(TU::B_THREADS);
     switch (mode) {
-      case -1: k_spec_rows<N, -1, false, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a); break;
-      case 0:
-        if (ptr) k_spec_rows<N, 0, true, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        else k_spec_rows<N, 0, false, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        break;
-      case 1:
-        if (ptr) k_spec_rows<N, 1, true, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        else k_spec_rows<N, 1, false, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        break;
-      default:
-        if (ptr) k_spec_rows<N, 2, true, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        else k_spec_rows<N, 2, false, TU><<<g, b, TU::B_SMEM_TOTAL, st>>>(a);
-        break;
+      case -1: launch<-1, false>(a, st); break;
+      case 0: ptr ? launch<0, true>(a, st) : launch<0, false>(a, st); break;
+      case 1: ptr ? launch<1, true>(a, st) : launch<1, false>(a, st); break;
+      default: ptr ? launch<2, true>(a, st) : launch<2, false>(a, st); break;
     }
   }
   static SpecVariant make(const char* name) { return SpecVariant{name, &set_attrs, &run}; }

@@ -98,3 +98,33 @@ def test_ensemble_autotune_restores_state_and_matches(pkg):
     finally:
         e.destroy()
         ref.destroy()
+
+
+@pytest.mark.parametrize("n", [512, 1024])
+def test_staged_row_shape_is_bitwise_its_unstaged_twin(pkg, n):
+    """The row shape that stages wcur / w0 / pointer force by bulk copy computes from the
+    same values in the same order as its twin that loads them from global memory: the
+    states agree bit for bit, with pointer forcing and stochastic forcing on."""
+    splat = {"x": 0.3, "y": 0.6, "dx": 0.02, "dy": -0.01, "color": (1.0, 0.5, 0.2), "radius": 0.04,
+             "amp": 3.0, "dyeAmp": 0.5}
+    outs = []
+    for staged in (False, True):
+        s = pkg.Solver.create(n=n, dyeScale=1)
+        try:
+            rep = s.autotune(steps=1)
+            names = [name for name, _ in rep["row"]]
+            twin = next(i for i, nm in enumerate(names) if nm.endswith("staged rows"))
+            plain = names.index(names[twin].replace(", staged rows", ""))
+            s.tuneSelect(0, twin if staged else plain)
+            s.configure(config(beta=5.0, drag=1e-2, viscosity=1.0, hyperP=4, forceAmp=0.2, forceK=n / 16,
+                               forceWidth=2.0, cfl=0.5, dtMax=1e-3))
+            s.reset({"k0": 10, "amplitude": 6, "seed": 5, "dyePattern": "none"})
+            s.setSplats([splat])
+            s.step(3, dye=False, reduce=True, graph=False, relatch=True)
+            s.setSplats([])
+            s.step(2, dye=False, reduce=True, graph=True, relatch=True)
+            outs.append((current_state(s), s.getBuffer("packA"), s.getBuffer("dt")))
+        finally:
+            s.destroy()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
