@@ -45,6 +45,7 @@ struct EnsInst {
   int n;
   int tiles_a, tiles_b;
   long long off;         // first cell in the pooled arrays
+  long long roff;        // first row in the pooled row flags
   const float2* tw;      // twiddle table of this n
 };
 
@@ -75,6 +76,9 @@ constexpr size_t kEnsBSmem = kEnsBBarOff + 16;
 struct Pools {
   float2* s[3];
   float2 *pa, *pb, *z;
+  // per instance row ky: 0 = the last row pass left PA/PB row ky all zero and unwritten
+  // (the column pass reads no such row); starts at "may be nonzero"
+  int* row_nz;
 };
 
 // MINB: resident CTAs per SM the register allocation must allow (a tuned choice)
@@ -91,6 +95,7 @@ __global__ void __launch_bounds__(kEnsAThreads, MINB)
     a.z = pool.z + I.off;
     a.params = &I.p;
     a.tw = I.tw;
+    a.row_nz = pool.row_nz + I.roff;
     switch (I.n) {
       case 64: phys_cols_tile<64, 1>(a, it.y, smem); break;
       case 128: phys_cols_tile<128, 1>(a, it.y, smem); break;
@@ -134,6 +139,7 @@ __global__ void __launch_bounds__(kEnsBThreads, MINB)
     a.tw = I.tw;
     a.stochastic = I.p.force_amp > 0.f ? 1 : 0;
     a.err = err;
+    a.row_nz = pool.row_nz + I.roff;
     switch (I.n) {
       case 64: spec_rows_tile<64, MODE, false>(a, it.y, smem, bar, parity); break;
       case 128: spec_rows_tile<128, MODE, false>(a, it.y, smem, bar, parity); break;
@@ -278,7 +284,7 @@ static void ens_free(s2d_ensemble* e) {
     if (kv.second.first) cudaGraphDestroy(kv.second.first);
   }
   void* ptrs[] = {e->dinst, e->dseeds, e->items_a, e->items_b, e->pool.s[0], e->pool.s[1], e->pool.s[2],
-                  e->pool.pa, e->pool.pb, e->pool.z, e->tw, e->sums, e->err};
+                  e->pool.pa, e->pool.pb, e->pool.z, e->pool.row_nz, e->tw, e->sums, e->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -333,7 +339,7 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
   // instances and work lists (largest grids first for balance)
   e->hinst.resize(count);
   e->seeds.resize(count);
-  long long off = 0;
+  long long off = 0, roff = 0;
   for (int i = 0; i < count; ++i) {
     const s2d_instance_desc& d = descs[i];
     EnsInst& I = e->hinst[i];
@@ -361,8 +367,10 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
       default: tiles_of<1024>(I.tiles_a, I.tiles_b); break;
     }
     I.off = off;
+    I.roff = roff;
     I.tw = e->tw + tw_off[n];
     off += (long long)n * n;
+    roff += n;
     e->seeds[i] = d.seed;
   }
   e->cells = off;
@@ -388,6 +396,8 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
   TRY(cudaMalloc(&e->pool.pa, cbytes), "pack pool");
   TRY(cudaMalloc(&e->pool.pb, cbytes), "pack pool");
   TRY(cudaMalloc(&e->pool.z, cbytes), "product pool");
+  TRY(cudaMalloc(&e->pool.row_nz, sizeof(int) * (size_t)roff), "row flags");
+  TRY(cudaMemsetAsync(e->pool.row_nz, 1, sizeof(int) * (size_t)roff, e->stream), "memset");   // nonzero words
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(e->pool.s[i], 0, cbytes, e->stream), "memset");
   TRY(cudaMemsetAsync(e->pool.z, 0, cbytes, e->stream), "memset");
   TRY(cudaMemcpyAsync(e->dinst, e->hinst.data(), sizeof(EnsInst) * count, cudaMemcpyHostToDevice, e->stream), "copy");
