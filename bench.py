@@ -7,16 +7,20 @@ Workload (the forced inverse-cascade configuration at 1024^2, FP32 FFT): one
 benchmark step is one substep of the reference's frame loop, i.e. one RK3 step
 (3 stages, 9 FFTs) + BFECC dye advection on the 2x refined 2048^2 dye grid +
 the CFL reduction; white-in-time stochastic forcing in the annulus |k| = 64+-2
-(amplitude 0.1), order-4 hyperviscosity nu4 = 1e-16, drag 1e-2, beta 0,
-CFL 0.5 capped at dt = 1e-3; seeded band-limited initial field (4 <= |k| <= 12,
-rms vorticity 1).  Inputs are synthetic and generated on the device.
+(amplitude 0.1), order-4 hyperviscosity with damping rate 1 at the dealias cutoff
+(nu4 = 5.4e-21; the written nu4 = 1e-16 overflows the FP32 integrating factor at the
+band corner), drag 1e-2, beta 0, CFL 0.5 capped at dt = 1e-3; seeded band-limited
+initial field (4 <= |k| <= 12, rms vorticity 1).  Inputs are synthetic and generated
+on the device.
 
 Rank 0 prints ONE JSON line.  ``value`` is device-timed whole-job steps/s
 (CUDA events on the solver stream, barrier + synchronize around the timed
 region, max over ranks; N ranks run N independent replicas: "replicas only",
 weak scaling).  ``e2e`` is the same metric through the public Solver API with
-per-step host->device parameter/splat uploads and a device->host diagnostics
-read inside the timed region.  ``roofline`` covers the dominant kernel,
+per-step host->device parameter/splat uploads (pinned host memory) and a
+device->host diagnostics read inside the timed region; reads run one step behind,
+as the reference's frame loop resolves its async readDiagnostics while the next
+frame runs, and the last step's read is inside the timed region too.  ``roofline`` covers the dominant kernel,
 ``cpu_baseline`` the FP64 NumPy restatement of reference/spectral2d.py on the
 host, ``ensemble`` the batched 256 x 256^2 ensemble, ``ensemble_mixed`` the mixed batch
 128 x 128^2 + 256 x 256^2 + 32 x 512^2.
