@@ -22,8 +22,10 @@ def test_read_before_copy_is_null(pkg):
         s.destroy()
 
 
-@pytest.mark.parametrize("n", [64, 512])
+@pytest.mark.parametrize("n", [32, 64, 512, 2048])
 def test_fp64_diagnostics(pkg, n):
+    """Every k-space tile geometry of the diagnostics kernel: a tile spanning the whole
+    grid (32), whole rows of both signs (64), and 64 x 32 tiles of one sign (512, 2048)."""
     s = pkg.Solver.create(n=n, dyeScale=1)
     try:
         s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
@@ -70,8 +72,8 @@ def test_zonal_mean_is_the_stage2_velocity(pkg):
         s.destroy()
 
 
-def test_fixed_point_diagnostics_match_restatement(pkg):
-    n = 128
+@pytest.mark.parametrize("n", [32, 128, 1024])
+def test_fixed_point_diagnostics_match_restatement(pkg, n):
     s = pkg.Solver.create(n=n, dyeScale=1)
     try:
         s.seed(k0=14, amplitude=6, seed=3)
