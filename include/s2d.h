@@ -326,6 +326,9 @@ int s2d_ensemble_energy(s2d_ensemble* e, double* energy, double* enstrophy);
  * drops captured step graphs.  The shapes differ in register allocation only. */
 int s2d_ensemble_autotune(s2d_ensemble* e, int steps, s2d_tune_report* report);
 int s2d_ensemble_tune_variant_name(s2d_ensemble* e, int kind, int index, char* out, int cap);
+/* Pin the column / row launch shapes (indices as in the report above; drops captured
+ * step graphs).  No reference counterpart. */
+int s2d_ensemble_tune_select(s2d_ensemble* e, int phys, int spec);
 
 #ifdef __cplusplus
 }

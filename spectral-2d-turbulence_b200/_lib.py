@@ -150,6 +150,7 @@ PROTOTYPES = {
     "s2d_ensemble_step": (_i, [_vp, _i, _i]),
     "s2d_ensemble_autotune": (_i, [_vp, _i, C.POINTER(s2d_tune_report)]),
     "s2d_ensemble_tune_variant_name": (_i, [_vp, _i, _i, C.c_char_p, _i]),
+    "s2d_ensemble_tune_select": (_i, [_vp, _i, _i]),
     "s2d_ensemble_energy": (_i, [_vp, C.POINTER(_d), C.POINTER(_d)]),
 }
 

@@ -111,7 +111,10 @@ __global__ void __launch_bounds__(kEnsAThreads, MINB)
 // larger than L2 the row pass waits on HBM, and more CTAs in flight hide more of it even
 // with some registers spilled to L1 (256 x 256^2: 761 -> 831 ensemble-steps/s going from
 // four CTAs at 128 registers to six at 80); s2d_ensemble_autotune picks per ensemble.
-template <int MODE, int MINB>
+// PAIR: the two inverse transforms of the next packs run as one two-line transform
+// (half the barrier-separated passes, twice the registers for them).
+template <int N, bool PAIR> using EnsTune = Tune<N, 16, 0, 0, false, PAIR>;
+template <int MODE, int MINB, bool PAIR = false>
 __global__ void __launch_bounds__(kEnsBThreads, MINB)
     k_ens_spec(const EnsInst* __restrict__ inst, const int2* __restrict__ items, int nitems, Pools pool, int phase,
                int* err) {
@@ -141,11 +144,11 @@ __global__ void __launch_bounds__(kEnsBThreads, MINB)
     a.err = err;
     a.row_nz = pool.row_nz + I.roff;
     switch (I.n) {
-      case 64: spec_rows_tile<64, MODE, false>(a, it.y, smem, bar, parity); break;
-      case 128: spec_rows_tile<128, MODE, false>(a, it.y, smem, bar, parity); break;
-      case 256: spec_rows_tile<256, MODE, false>(a, it.y, smem, bar, parity); break;
-      case 512: spec_rows_tile<512, MODE, false>(a, it.y, smem, bar, parity); break;
-      default: spec_rows_tile<1024, MODE, false>(a, it.y, smem, bar, parity); break;
+      case 64: spec_rows_tile<64, MODE, false, EnsTune<64, PAIR>>(a, it.y, smem, bar, parity); break;
+      case 128: spec_rows_tile<128, MODE, false, EnsTune<128, PAIR>>(a, it.y, smem, bar, parity); break;
+      case 256: spec_rows_tile<256, MODE, false, EnsTune<256, PAIR>>(a, it.y, smem, bar, parity); break;
+      case 512: spec_rows_tile<512, MODE, false, EnsTune<512, PAIR>>(a, it.y, smem, bar, parity); break;
+      default: spec_rows_tile<1024, MODE, false, EnsTune<1024, PAIR>>(a, it.y, smem, bar, parity); break;
     }
     __syncthreads();
   }
@@ -153,24 +156,26 @@ __global__ void __launch_bounds__(kEnsBThreads, MINB)
 
 // ---- launch-shape variants of the two persistent stage kernels (index 0 = default)
 constexpr int kEnsPhysMinb[] = {2, 3};      // resident CTAs per SM of each shape
-constexpr int kEnsSpecMinb[] = {6, 4, 5};
-constexpr int kEnsNPhys = 2, kEnsNSpec = 3;
+constexpr int kEnsSpecMinb[] = {6, 4, 5, 4};
+constexpr bool kEnsSpecPair[] = {false, false, false, true};
+constexpr int kEnsNPhys = 2, kEnsNSpec = 4;
 
 template <int MINB> cudaError_t ens_phys_attrs() {
   return cudaFuncSetAttribute(k_ens_phys<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsASmem);
 }
-template <int MINB> cudaError_t ens_spec_attrs() {
-  cudaError_t e = cudaFuncSetAttribute(k_ens_spec<-1, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<0, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<1, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<2, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+template <int MINB, bool PAIR = false> cudaError_t ens_spec_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_ens_spec<-1, MINB, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<0, MINB, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<1, MINB, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_spec<2, MINB, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsBSmem);
   return e;
 }
 const void* ens_phys_fn(int v) {
   return v == 1 ? (const void*)k_ens_phys<3> : (const void*)k_ens_phys<2>;
 }
 const void* ens_spec_fn(int v) {
-  return v == 1 ? (const void*)k_ens_spec<1, 4> : v == 2 ? (const void*)k_ens_spec<1, 5> : (const void*)k_ens_spec<1, 6>;
+  return v == 1 ? (const void*)k_ens_spec<1, 4> : v == 2 ? (const void*)k_ens_spec<1, 5>
+         : v == 3 ? (const void*)k_ens_spec<1, 4, true> : (const void*)k_ens_spec<1, 6>;
 }
 void ens_launch_phys(int v, int grid, cudaStream_t st, const EnsInst* inst, const int2* items, int nitems, Pools pool) {
   if (v == 1) k_ens_phys<3><<<grid, kEnsAThreads, kEnsASmem, st>>>(inst, items, nitems, pool);
@@ -181,6 +186,8 @@ void ens_launch_spec_m(int v, int grid, cudaStream_t st, const EnsInst* inst, co
                        int phase, int* err) {
   if (v == 1) k_ens_spec<MODE, 4><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
   else if (v == 2) k_ens_spec<MODE, 5><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
+  else if (v == 3)
+    k_ens_spec<MODE, 4, true><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
   else k_ens_spec<MODE, 6><<<grid, kEnsBThreads, kEnsBSmem, st>>>(inst, items, nitems, pool, phase, err);
 }
 void ens_launch_spec(int mode, int v, int grid, cudaStream_t st, const EnsInst* inst, const int2* items, int nitems,
@@ -409,6 +416,7 @@ extern "C" int s2d_ensemble_create(const s2d_instance_desc* descs, int count, in
   TRY(ens_spec_attrs<4>(), "attr");
   TRY(ens_spec_attrs<5>(), "attr");
   TRY(ens_spec_attrs<6>(), "attr");
+  TRY((ens_spec_attrs<4, true>()), "attr");
   for (int v = 0; v < kEnsNPhys; ++v) {
     int occ = 0;
     TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_phys_fn(v), kEnsAThreads, kEnsASmem), "occupancy");
@@ -568,7 +576,8 @@ extern "C" int s2d_ensemble_tune_variant_name(s2d_ensemble* e, int kind, int ind
   if (!out || cap <= 0) return efail(S2D_ERR_ARG, "output is null");
   const int count = kind == 0 ? kEnsNPhys : kind == 1 ? kEnsNSpec : -1;
   if (count < 0 || index < 0 || index >= count) return efail(S2D_ERR_ARG, "variant out of range");
-  std::snprintf(out, (size_t)cap, "%d CTAs/SM", kind == 0 ? kEnsPhysMinb[index] : kEnsSpecMinb[index]);
+  std::snprintf(out, (size_t)cap, "%d CTAs/SM%s", kind == 0 ? kEnsPhysMinb[index] : kEnsSpecMinb[index],
+                kind == 1 && kEnsSpecPair[index] ? ", paired inverse transforms" : "");
   return S2D_OK;
 }
 
@@ -644,6 +653,20 @@ extern "C" int s2d_ensemble_autotune(s2d_ensemble* e, int steps, s2d_tune_report
   rep.phys_choice = e->pv;
   rep.spec_choice = e->sv;
   if (report) *report = rep;
+  return S2D_OK;
+}
+
+extern "C" int s2d_ensemble_tune_select(s2d_ensemble* e, int phys, int spec) {
+  E_USE(e);
+  if (phys < 0 || phys >= kEnsNPhys || spec < 0 || spec >= kEnsNSpec)
+    return efail(S2D_ERR_ARG, "ensemble shape index out of range");
+  e->pv = phys;
+  e->sv = spec;
+  for (auto& kv : e->graphs) {          // captured with the previous shapes
+    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+  }
+  e->graphs.clear();
   return S2D_OK;
 }
 

@@ -28,10 +28,12 @@ namespace s2d {
 // Launch shape of the stage kernels for N x N: V values per thread (T = N/V threads per
 // line; the line FFT runs radix-V passes), GA columns per column-kernel CTA, PPB row pairs
 // per row-kernel CTA, the resident CTAs the register budget must allow (AMB_/BMB_;
-// 0 = as many as 128 registers a thread give), and whether the row kernel stages the
-// rows its RK update reads by bulk copy (PF_).  Tune<N> is the default shape; the
+// 0 = as many as 128 registers a thread give), whether the row kernel stages the
+// rows its RK update reads by bulk copy (PF_), and whether it runs the two inverse
+// x-transforms of the next packs as one two-line transform (PAIR_: half the
+// barrier-separated passes, twice the registers).  Tune<N> is the default shape; the
 // autotuner picks among the variants each size registers (s2d_ops.cuh).
-template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0, bool PF_ = false> struct Tune {
+template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0, bool PF_ = false, bool PAIR_ = false> struct Tune {
   static constexpr int N = N_;
   static constexpr int V = V_;
   static constexpr int T = N / V;
@@ -59,6 +61,7 @@ template <int N_, int V_ = 16, int AMB_ = 0, int BMB_ = 0, bool PF_ = false> str
   // staging is sized per kernel instance (spec_smem): 16 KB a row pair per array at
   // 1024^2, so the stage kernels without pointer forcing keep 3 CTAs per SM.
   static constexpr bool PREFETCH = PF_;
+  static constexpr bool PAIR_IFFT = PAIR_;
   static constexpr size_t B_BAR_OFF = B_SMEM;
   static constexpr size_t B_STAGE_OFF = B_SMEM + 16;
   static constexpr size_t B_SMEM_TOTAL = B_STAGE_OFF;   // without staging
@@ -399,6 +402,32 @@ __device__ __forceinline__ void spec_rows_tile(const SpecArgs& a, int tile, floa
   // next-stage packs, scaled by the 1/N^2 of the inverse 2D transform, x-IFFT each;
   // the two transforms share one code path
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  if constexpr (TU::PAIR_IFFT) {
+    // both packs formed first, then one two-line transform through own0 and own1 (the
+    // same arithmetic per line as the one-line transforms below)
+    float2 x[2][V];
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      const int c = t + T * m;
+      const float kx = wn<N>(c);
+      const float k2 = kx * kx + ky * ky;
+      const float inv = k2 > 0.f ? __frcp_rn(k2) : 0.f;
+      const float2 w = own1[PL::pad(c)];
+      const float fa = (1.f - ky * inv) * inv_n2;       // w + i u_hat = w (1 - ky/k2)
+      const float fb = kx * inv * inv_n2;                // v_hat = -i kx w / k2
+      x[0][m] = make_float2(w.x * fa, w.y * fa);
+      x[1][m] = make_float2(w.y * fb, -w.x * fb);
+    }
+    __syncthreads();   // every thread's own1 reads done before the transform writes own1
+    float2* const xb[2] = {own0, own1};
+    fft_lines<N, V, +1, 2>(x, xb, t, a.tw, CtaSync{});
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      a.pa[rbase + t + T * m] = x[0][m];
+      a.pb[rbase + t + T * m] = x[1][m];
+    }
+    return;
+  }
 #pragma unroll 1
   for (int q = 0; q < 2; ++q) {
     float2 x[1][V];

@@ -8,7 +8,8 @@ const NOps* ops_n1024() {
   static const NOps o = OpsImpl<1024>::make({PhysImpl<1024, Tune<1024, 8, 2>>::make("V=8, 2 CTAs/SM")},
                                        {SpecImpl<1024, Tune<1024, 8, 0, 4>>::make("V=8, 4 CTAs/SM"),
                                         SpecImpl<1024, Tune<1024, 8, 0, 3>>::make("V=8, 3 CTAs/SM"),
-                                        SpecImpl<1024, Tune<1024, 8, 0, 3, true>>::make("V=8, 3 CTAs/SM, staged rows")});
+                                        SpecImpl<1024, Tune<1024, 8, 0, 3, false, true>>::make(
+                                            "V=8, 3 CTAs/SM, paired inverse transforms")});
   return &o;
 }
 }  // namespace s2d

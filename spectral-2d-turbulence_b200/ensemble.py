@@ -71,13 +71,18 @@ class Ensemble:
         L.call("s2d_ensemble_autotune", self._h, int(steps), C.byref(rep))
 
         def name(kind, i):
-            buf = C.create_string_buffer(32)
-            L.call("s2d_ensemble_tune_variant_name", self._h, kind, i, buf, 32)
+            buf = C.create_string_buffer(64)
+            L.call("s2d_ensemble_tune_variant_name", self._h, kind, i, buf, 64)
             return buf.value.decode()
         col = [(name(0, i), float(rep.phys_us[i])) for i in range(rep.phys_variants)]
         row = [(name(1, i), float(rep.spec_us[i])) for i in range(rep.spec_variants)]
         return {"column": col, "row": row,
                 "choice": {"column": col[rep.phys_choice][0], "row": row[rep.spec_choice][0]}}
+
+    def tuneSelect(self, column: int, row: int):
+        """Pin the column / row shapes (indices into autotune()'s lists); no reference
+        counterpart."""
+        L.call("s2d_ensemble_tune_select", self._h, int(column), int(row))
 
     def synchronize(self):
         L.call("s2d_ensemble_synchronize", self._h)

@@ -86,7 +86,7 @@ def test_ensemble_autotune_restores_state_and_matches(pkg):
         ref.step(2, graph=False)
         before = [e.getState(i) for i in range(e.count)]
         rep = e.autotune(2)
-        assert len(rep["column"]) == 2 and len(rep["row"]) == 3
+        assert len(rep["column"]) == 2 and len(rep["row"]) == 4
         assert all(us > 0 for _, us in rep["column"] + rep["row"])
         for i in range(e.count):
             assert np.array_equal(e.getState(i), before[i])
@@ -100,11 +100,13 @@ def test_ensemble_autotune_restores_state_and_matches(pkg):
         ref.destroy()
 
 
-@pytest.mark.parametrize("n", [512, 1024])
-def test_staged_row_shape_is_bitwise_its_unstaged_twin(pkg, n):
-    """The row shape that stages wcur / w0 / pointer force by bulk copy computes from the
-    same values in the same order as its twin that loads them from global memory: the
-    states agree bit for bit, with pointer forcing and stochastic forcing on."""
+@pytest.mark.parametrize("n,suffix", [(512, "staged rows"), (1024, "paired inverse transforms")])
+def test_derived_row_shape_matches_its_twin(pkg, n, suffix):
+    """A row shape derived from another one, with pointer forcing and stochastic forcing
+    on.  Staging wcur / w0 / pointer force by bulk copy changes only where the same values
+    are loaded from: the states agree bit for bit.  Running the two inverse transforms
+    of the next packs as one two-line transform is the same arithmetic, but the compiler
+    may contract its multiply-adds differently: the states agree to FP32 rounding."""
     splat = {"x": 0.3, "y": 0.6, "dx": 0.02, "dy": -0.01, "color": (1.0, 0.5, 0.2), "radius": 0.04,
              "amp": 3.0, "dyeAmp": 0.5}
     outs = []
@@ -113,8 +115,8 @@ def test_staged_row_shape_is_bitwise_its_unstaged_twin(pkg, n):
         try:
             rep = s.autotune(steps=1)
             names = [name for name, _ in rep["row"]]
-            twin = next(i for i, nm in enumerate(names) if nm.endswith("staged rows"))
-            plain = names.index(names[twin].replace(", staged rows", ""))
+            twin = next(i for i, nm in enumerate(names) if nm.endswith(suffix))
+            plain = names.index(names[twin].replace(", " + suffix, ""))
             s.tuneSelect(0, twin if staged else plain)
             s.configure(config(beta=5.0, drag=1e-2, viscosity=1.0, hyperP=4, forceAmp=0.2, forceK=n / 16,
                                forceWidth=2.0, cfl=0.5, dtMax=1e-3))
@@ -126,5 +128,35 @@ def test_staged_row_shape_is_bitwise_its_unstaged_twin(pkg, n):
             outs.append((current_state(s), s.getBuffer("packA"), s.getBuffer("dt")))
         finally:
             s.destroy()
-    for a, b in zip(outs[0], outs[1]):
-        assert np.array_equal(a, b)
+    if suffix == "staged rows":
+        for a, b in zip(outs[0], outs[1]):
+            assert np.array_equal(a, b)
+    else:
+        assert rel_l2(outs[1][0], outs[0][0]) <= 1e-6
+        assert rel_l2(outs[1][1], outs[0][1]) <= 1e-6
+        assert abs(float(outs[1][2][0]) / float(outs[0][2][0]) - 1.0) <= 1e-5
+
+
+def test_every_ensemble_shape_matches_the_default(pkg):
+    """Each registered launch shape of the persistent ensemble kernels (resident CTAs,
+    paired inverse transforms) steps the mixed ensemble like the default shape, to FP32
+    rounding (the paired transform may contract multiply-adds differently)."""
+    ref = _mixed_ensemble(pkg)
+    try:
+        ref.step(4, graph=True)
+        want = [ref.getState(i) for i in range(ref.count)]
+        rep = ref.autotune(1)
+        names = [nm for nm, _ in rep["row"]]
+        assert any(nm.endswith("paired inverse transforms") for nm in names)
+    finally:
+        ref.destroy()
+    for col in range(len(rep["column"])):
+        for row in range(len(rep["row"])):
+            e = _mixed_ensemble(pkg)
+            try:
+                e.tuneSelect(col, row)
+                e.step(4, graph=True)
+                for i in range(e.count):
+                    assert rel_l2(e.getState(i), want[i]) <= 1e-6, (rep["column"][col][0], names[row], i)
+            finally:
+                e.destroy()
