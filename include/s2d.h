@@ -284,8 +284,9 @@ int s2d_profile_read(s2d_solver* s, double* ms /* S2D_PROF_CLASSES */, int* laun
  * static device array of S2D_CFL_STATIC_MAX_PARTIALS floats (16 KiB) that every
  * GPU loading the library holds until the process exits, so n is limited to
  * S2D_CFL_STATIC_MAX_N; larger n is rejected with S2D_ERR_ARG.  The first call
- * on a device looks up that array's device address (cudaGetSymbolAddress) with
- * the device current; make that first call before any stream capture.  All
+ * in each CUDA context (a device's primary context, or a context the caller made
+ * current) looks up that array's device address there (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All
  * calls on a device share the array: calls that overlap on the GPU (other
  * streams, other host threads) race and must be ordered by the caller. */
 #define S2D_CFL_STATIC_MAX_N 4096
@@ -296,7 +297,7 @@ int s2d_cfl_dt_static(const void* vel, int n, float cfl, float dt_min, float dt_
 /* Many independent instances of uneven sizes stepped together (no reference
  * counterpart beyond running many Solvers; BASELINE batching form). */
 typedef struct s2d_instance_desc {
-  int32_t n;              /* 32..512, power of two */
+  int32_t n;              /* 64..1024, power of two */
   float beta, drag, nu_h; /* nu_h directly (not the rate) */
   int32_t hyper_p;
   float dt;               /* fixed step of this instance */

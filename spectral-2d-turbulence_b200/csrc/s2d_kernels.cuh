@@ -228,6 +228,7 @@ __device__ __forceinline__ void cols_speed_finalize(const PhysArgs& a, float spe
   }
   __syncthreads();
   if (last) {
+    __threadfence();   // acquire side of the ticket: the other CTAs' partials are read after it
     float s = 0.f;
     for (int i = tid; i < (int)gridDim.x; i += blockDim.x) s = fmaxf(s, __ldcg(a.partials + i));
     s = warp_max(s);

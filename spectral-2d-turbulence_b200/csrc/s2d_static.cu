@@ -8,6 +8,7 @@
 // caller passes the velocity field and the two-float result buffer; the only
 // scratch is the partial-maximum array below, a static device array that every
 // GPU loading this library holds until the process exits.
+#include <cuda.h>   // CUcontext / CUresult types only; the functions come from cudaGetDriverEntryPoint
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -71,33 +72,89 @@ __global__ void k_static_dt(const float* __restrict__ partials, int count, float
   }
 }
 
-// device address of the static scratch, looked up once per device
-constexpr int kMaxDevices = 64;
-std::mutex g_addr_mutex;
-float* g_addr[kMaxDevices] = {nullptr};
+// Device address of the static scratch, looked up once per CUDA context.  The array
+// lives in the module loaded into a context, so its address belongs to that context:
+// after cudaDeviceReset (the primary context is destroyed and a new one created) or
+// with another driver-API context current, the address cached for an earlier context
+// would be a dead or foreign pointer.  The cache is therefore keyed on the unique
+// context id of the driver (cuCtxGetId), reached through cudaGetDriverEntryPoint so
+// the library does not link libcuda.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
 
-int scratch_for_current_device(float** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    s2d::ens_set_error(std::string("s2d_cfl_dt_static: cudaGetDevice: ") + cudaGetErrorString(e));
-    return S2D_ERR_NO_DEVICE;
+struct ScratchSlot {
+  unsigned long long ctx_id;
+  float* addr;
+};
+constexpr int kCacheSlots = 64;
+std::mutex g_addr_mutex;
+ScratchSlot g_slots[kCacheSlots];
+int g_slots_used = 0, g_slot_next = 0;
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+
+int resolve_driver_entry_points() {
+  if (g_ctx_get_current && g_ctx_get_id) return S2D_OK;
+  void* f1 = nullptr;
+  void* f2 = nullptr;
+  cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+  cudaError_t e1 = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1);
+  cudaError_t e2 = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+      q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+    s2d::ens_set_error("s2d_cfl_dt_static: the driver does not provide cuCtxGetCurrent/cuCtxGetId");
+    return S2D_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    s2d::ens_set_error("s2d_cfl_dt_static: device ordinal out of range");
-    return S2D_ERR_ARG;
+  g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(f1);
+  g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(f2);
+  return S2D_OK;
+}
+
+int symbol_address(float** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_cfl_partials);
+  if (e != cudaSuccess || !p) {
+    s2d::ens_set_error(std::string("s2d_cfl_dt_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return S2D_ERR_CUDA;
   }
+  *out = static_cast<float*>(p);
+  return S2D_OK;
+}
+
+int scratch_for_current_context(float** out) {
   std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_cfl_partials);
-    if (e != cudaSuccess || !p) {
-      s2d::ens_set_error(std::string("s2d_cfl_dt_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return S2D_ERR_CUDA;
-    }
-    g_addr[dev] = static_cast<float*>(p);
+  if (int rc = resolve_driver_entry_points()) return rc;
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) {
+    s2d::ens_set_error("s2d_cfl_dt_static: cuCtxGetCurrent failed");
+    return S2D_ERR_CUDA;
   }
-  *out = g_addr[dev];
+  if (!ctx) {
+    // no context current yet on this thread: the runtime call creates the current
+    // device's primary context and makes it current
+    float* p = nullptr;
+    if (int rc = symbol_address(&p)) return rc;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) {
+      s2d::ens_set_error("s2d_cfl_dt_static: no CUDA context is current");
+      return S2D_ERR_NO_DEVICE;
+    }
+  }
+  unsigned long long id = 0;
+  if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) {
+    s2d::ens_set_error("s2d_cfl_dt_static: cuCtxGetId failed");
+    return S2D_ERR_CUDA;
+  }
+  for (int i = 0; i < g_slots_used; ++i)
+    if (g_slots[i].ctx_id == id) {
+      *out = g_slots[i].addr;
+      return S2D_OK;
+    }
+  float* p = nullptr;
+  if (int rc = symbol_address(&p)) return rc;
+  // a context not seen before: remember it (the oldest entry makes room when full)
+  const int slot = g_slots_used < kCacheSlots ? g_slots_used++ : (g_slot_next++ % kCacheSlots);
+  g_slots[slot] = {id, p};
+  *out = p;
   return S2D_OK;
 }
 
@@ -115,7 +172,7 @@ extern "C" int s2d_cfl_dt_static(const void* vel, int n, float cfl, float dt_min
     return S2D_ERR_ARG;
   }
   float* partials = nullptr;
-  if (int rc = scratch_for_current_device(&partials)) return rc;
+  if (int rc = scratch_for_current_context(&partials)) return rc;
   const long long cells = (long long)n * n;
   const int parts = (int)((cells + kCellsPerPartial - 1) / kCellsPerPartial);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
