@@ -22,7 +22,7 @@ device->host diagnostics read inside the timed region; reads run one step behind
 as the reference's frame loop resolves its async readDiagnostics while the next
 frame runs, and the last step's read is inside the timed region too.  ``roofline`` covers the dominant kernel,
 ``cpu_baseline`` the FP64 NumPy restatement of reference/spectral2d.py on the
-host, ``ensemble`` the batched 256 x 256^2 ensemble, ``ensemble_mixed`` the mixed batch
+host started from the GPU arm's own initial field, ``ensemble`` the batched 256 x 256^2 ensemble, ``ensemble_mixed`` the mixed batch
 128 x 128^2 + 256 x 256^2 + 32 x 512^2.
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port of
@@ -277,16 +277,22 @@ def shard_by_cost(instances, world):
 
 # ------------------------------------------------------------------ CPU reference arm
 def _oracle_worker(args):
-    """Run `steps` oracle RK3 steps on the workload; returns (steps, seconds)."""
-    n, steps, seed = args
+    """Run `steps` oracle RK3 steps on the workload; returns (steps, seconds).
+
+    The initial field is `w0` when given (the GPU arm's own initial state, read back from
+    the device), else the CPU restatement of the device band seed s2d_seed_band with the
+    GPU arm's seed (1 + rank), so both arms start from the same FP32 field."""
+    n, steps, seed, w0 = args
     import numpy as np
     from oracle import wgsl_oracle as wo
-    from oracle.spectral_oracle import SpectralOracle, band_noise_spectrum
+    from oracle.spectral_oracle import SpectralOracle
     nu_h = float(wo.nu_h_from_rate(CFG["viscosity"], n, HYPER_P))
     s = SpectralOracle(n=n, beta=CFG["beta"], mu=CFG["drag"], nu_h=nu_h, hyper_p=HYPER_P, cfl=CFG["cfl"],
                        dt_max=CFG["dtMax"])
-    s.w = band_noise_spectrum(n, 4, 12, seed)
+    init = w0 if w0 is not None else wo.band_seed_spectrum(n, 4.0, 12.0, 1.0, seed)
+    s.w = np.asarray(init).astype(np.complex128)
     s.step(dt=CFG["dtMax"])        # warm-up
+    s.w = np.asarray(init).astype(np.complex128)
     t0 = time.perf_counter()
     for k in range(steps):
         dt = s.timestep()
@@ -295,14 +301,16 @@ def _oracle_worker(args):
     return steps, time.perf_counter() - t0
 
 
-def cpu_baseline(budget_s=15.0):
-    """The FP64 NumPy restatement of reference/spectral2d.py, one core, bounded sample."""
-    steps1, t1 = _oracle_worker((N, 1, 0))
+def cpu_baseline(w0, budget_s=15.0):
+    """The FP64 NumPy restatement of reference/spectral2d.py, one core, bounded sample,
+    started from the GPU arm's own initial field `w0` (the same FP32 bits)."""
+    steps1, t1 = _oracle_worker((N, 1, 1, w0))
     k = max(1, min(20, int(budget_s / max(t1, 1e-3))))
-    steps, secs = _oracle_worker((N, k, 0))
+    steps, secs = _oracle_worker((N, k, 1, w0))
     return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{steps} RK3 steps of one {N}^2 instance with forcing and CFL dt "
-                      f"(FP64 NumPy restatement of reference/spectral2d.py, no dye), {secs:.1f} s"}
+                      f"(FP64 NumPy restatement of reference/spectral2d.py, no dye), {secs:.1f} s; "
+                      "initial field = the GPU arm's seeded state read back from the device (same FP32 bits)"}
 
 
 def run_reference(args):
@@ -312,12 +320,12 @@ def run_reference(args):
         return 0
     procs = max(1, min(os.cpu_count() or 1, 16))
     # bound the run: each replica does at most what fits ~90 s of host time
-    _, t1 = _oracle_worker((N, 1, 0))
+    _, t1 = _oracle_worker((N, 1, 1, None))
     per = max(1, min(args.steps, int(90.0 / max(t1, 1e-3))))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_oracle_worker, [(N, per, r) for r in range(procs)])
+        res = pool.map(_oracle_worker, [(N, per, 1 + r, None) for r in range(procs)])
     wall = time.perf_counter() - t0
     steps = sum(r[0] for r in res)
     secs = max(r[1] for r in res)
@@ -349,6 +357,7 @@ def run_ours(args):
     solver.configure(CFG)
     solver.reset({"k0": 14, "amplitude": 0, "seed": 1, "dyePattern": "bands"})
     solver.seedBand(4.0, 12.0, rms=1.0, seed=1 + rank)
+    w_init = solver.getBuffer("state0") if (rank == 0 and world == 1 and not args.no_cpu) else None
     stream = torch.cuda.ExternalStream(solver.stream, device=dev)
     # stage-kernel launch shapes chosen by the library's autotuner (before any timing), or
     # pinned with --shapes (reproducible profiling)
@@ -461,7 +470,7 @@ def run_ours(args):
         ens = run_ensemble(pkg, torch, world, rank, dev, args)
         ens_mixed = run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_MIXED, seed=4321)
 
-    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(w_init) if w_init is not None else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -600,7 +609,7 @@ ENSEMBLE_MIXED = ((128, 128), (256, 256), (512, 32))
 def run_ensemble(pkg, torch, world, rank, dev, args, groups=ENSEMBLE_256, seed=1234):
     """Graph-replayed RK3 steps of a batch of independent instances (sizes `groups` =
     (n, count) pairs), per-instance nu ~ U[1e-4, 1e-3], beta ~ U[0, 20], drag ~ U[0, 2e-2],
-    band-limited initial fields; instances sharded round-robin across ranks."""
+    band-limited initial fields; instances sharded by cost (N^2 log2 N, shard_by_cost) across ranks."""
     import numpy as np
     rng = np.random.default_rng(seed)
     inst = []

@@ -132,6 +132,14 @@ int s2d_set_sim_time(s2d_solver* s, double t);
 /* CUDA stream the solver enqueues on (cudaStream_t as void*). */
 int s2d_get_stream(s2d_solver* s, void** stream);
 int s2d_synchronize(s2d_solver* s);
+/* Failure-detection check (no reference counterpart; the reference's WebGPU queue has no
+ * device-side waits).  Every device-side wait of the library (bulk-copy and MMA
+ * barriers) gives up after a global-timer limit (50 ms), records its site in the
+ * solver's error word and lets the kernel return; the next s2d_synchronize (or any call
+ * that reads the word) returns S2D_ERR_CUDA.  This enqueues one CTA whose wait can
+ * never complete (its barrier expects bytes that are never sent), with a limit of
+ * limit_ns (1..1e9), so that path can be exercised without faulting the GPU. */
+int s2d_probe_wait_timeout(s2d_solver* s, unsigned long long limit_ns);
 
 /* ---------------------------------------------------------------- parameters */
 int s2d_configure(s2d_solver* s, const s2d_params* p);                   /* solver.js:306-324 */

@@ -327,3 +327,43 @@ def dye_step(dye_bits, vel, dt, fade, splats=()):
         res[..., :3] = (res[..., :3] + col[None, None, :] * wgt[..., None]).astype(F32)
     res[..., 3] = F32(1.0)
     return res.astype(np.float16).view(np.uint16)
+
+
+# ----------------------------------------------------------------------------- band seed
+def band_seed_spectrum(n, kmin, kmax, rms, seed):
+    """Restatement of the library's band-limited seed (s2d_seed_band; no reference
+    counterpart -- the benchmark configurations describe the field: complex Gaussian
+    noise in kmin <= |k| <= kmax, Hermitian-symmetrised, dealiased, k = 0 removed, rms
+    vorticity `rms`).  Cell (row, col) draws a complex Gaussian g by Box-Muller over
+    two hash1 values of (seed, row*n + col), evaluated in FP64 and rounded to FP32;
+    w = (g(k) + conj g(-k)) / 2 inside the band; then w *= rms / (sqrt(sum |w|^2) / n^2)
+    in FP64 with one FP32 rounding.  Returns complex64 (n, n).
+    """
+    idx = np.arange(n * n, dtype=np.uint64).astype(U32)
+
+    def gauss(i):
+        h1 = hash1(i ^ hash1(U32(seed) ^ U32(0x68BC21EB)))
+        h2 = hash1(h1 ^ U32(0x02E5BE93))
+        u1 = (h1.astype(np.float64) + 0.5) * (1.0 / 4294967296.0)
+        u2 = h2.astype(np.float64) * (1.0 / 4294967296.0)
+        r = np.sqrt(-2.0 * np.log(u1))
+        ang = np.pi * (2.0 * u2)
+        return (r * np.cos(ang)).astype(F32), (r * np.sin(ang)).astype(F32)
+
+    ax, ay = gauss(idx)
+    row = (idx // U32(n)).astype(np.int64)
+    col = (idx % U32(n)).astype(np.int64)
+    pidx = (((n - row) % n) * n + ((n - col) % n)).astype(np.uint64).astype(U32)
+    bx, by = gauss(pidx)
+    kx = np.where(col < n // 2, col, col - n).astype(F32)
+    ky = np.where(row < n // 2, row, row - n).astype(F32)
+    kr = np.sqrt(kx * kx + ky * ky).astype(F32)
+    kcut = F32(n / 3.0)
+    inside = (kr != 0) & (kr >= F32(kmin)) & (kr <= F32(kmax)) & (np.abs(kx) < kcut) & (np.abs(ky) < kcut)
+    wx = np.where(inside, F32(0.5) * (ax + bx), F32(0.0)).astype(F32)
+    wy = np.where(inside, F32(0.5) * (ay - by), F32(0.0)).astype(F32)
+    total = np.sum(wx.astype(np.float64) ** 2 + wy.astype(np.float64) ** 2)
+    cur = np.sqrt(total) / (float(n) * float(n))
+    sc = rms / cur if cur > 0 else 1.0
+    out = (wx.astype(np.float64) * sc).astype(F32) + 1j * (wy.astype(np.float64) * sc).astype(F32)
+    return out.astype(np.complex64).reshape(n, n)

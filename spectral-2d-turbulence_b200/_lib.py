@@ -140,6 +140,7 @@ PROTOTYPES = {
     "s2d_profile": (_i, [_vp, _i]),
     "s2d_profile_read": (_i, [_vp, C.POINTER(_d), C.POINTER(_i)]),
     "s2d_cfl_dt_static": (_i, [_vp, _i, _f, _f, _f, _vp, _vp]),
+    "s2d_probe_wait_timeout": (_i, [_vp, C.c_ulonglong]),
     "s2d_ensemble_create": (_i, [C.POINTER(s2d_instance_desc), _i, _i, C.POINTER(_vp)]),
     "s2d_ensemble_destroy": (_i, [_vp]),
     "s2d_ensemble_get_stream": (_i, [_vp, C.POINTER(_vp)]),

@@ -576,8 +576,33 @@ static int check_device_error(s2d_solver* s) {
   S2D_CUDA(cudaStreamSynchronize(s->stream));
   if (h) {
     cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
-    return fail(S2D_ERR_CUDA, "a device-side wait for staged rows timed out; results of that step are invalid");
+    return fail(S2D_ERR_CUDA, "a bounded device-side wait gave up (site " + std::to_string(h) +
+                                  "); results of the work enqueued since the last check are invalid");
   }
+  return S2D_OK;
+}
+
+// One CTA whose barrier expects 16 bytes that no copy ever delivers: its bounded wait
+// gives up after limit_ns, records site 5 in the error word and the kernel returns.
+// Nothing is in flight when it exits (no copy was issued), so the context stays usable.
+static __global__ void k_wait_probe(int* err, unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16u);
+  __syncthreads();
+  mbar_wait_bounded(&bar, 0u, err, 5, limit_ns);
+}
+
+extern "C" int s2d_probe_wait_timeout(s2d_solver* s, unsigned long long limit_ns) {
+  S2D_USE(s);
+  if (limit_ns == 0 || limit_ns > 1000000000ull) return fail(S2D_ERR_ARG, "limit_ns must be in 1..1e9");
+  DeviceGuard guard(s->dev);
+  k_wait_probe<<<1, 32, 0, s->stream>>>(s->err, limit_ns);
+  S2D_CUDA(cudaGetLastError());
   return S2D_OK;
 }
 

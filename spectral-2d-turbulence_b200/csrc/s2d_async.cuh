@@ -47,13 +47,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for phase `parity` of the barrier, giving up after ~2^24 polls (each poll
-// suspends in hardware for a bounded time).  On giving up, records `code` in the
-// device error word and returns false; the caller's results are then invalid
-// and the host reports the error at its next synchronization.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int code) {
-  for (uint32_t i = 0; i < (1u << 24); ++i)
+// nanoseconds of the GPU's global timer
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// default limit of a device-side wait: far above any legitimate wait in these kernels
+// (a bulk copy or an MMA group of microseconds), short enough that a wait that can never
+// end returns well inside a host-side timeout
+constexpr uint64_t kWaitLimitNs = 50ull * 1000ull * 1000ull;   // 50 ms
+
+// Wait for phase `parity` of the barrier for at most `limit_ns` of global-timer time.
+// On giving up, records `code` in the device error word and returns false; the
+// caller's results are then invalid and the host reports the error at its next
+// synchronization (s2d_synchronize / any call that reads the error word).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int code,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > limit_ns) break;
+  }
   if (err) atomicExch(err, code);
   return false;
 }

@@ -198,6 +198,11 @@ class Solver:
     def synchronize(self):
         L.call("s2d_synchronize", self._use())
 
+    def probeWaitTimeout(self, limit_ns: int):
+        """Enqueue one CTA whose bounded device wait cannot complete (failure-detection
+        check): the next synchronize() raises S2DError with S2D_ERR_CUDA."""
+        L.call("s2d_probe_wait_timeout", self._use(), int(limit_ns))
+
     # ---------------------------------------------------------------- parameters
     def configure(self, cfg: dict):
         """solver.js:306-324: latches stepIndex for the stochastic forcing phase."""

@@ -2,9 +2,9 @@
 
 Run in a container where the reference checkout is available::
 
-    python tests/golden/make_golden.py [path/to/reference]
+    python tests/golden/make_golden.py path/to/reference
 
-(default path: /root/reference).  It
+(or set S2D_REFERENCE to the checkout and pass no argument).  It
 
 * re-exports the reference's own golden vectors ``tests/fixtures.json``
   (N=32: fft, velocity packing, assembly, one step, twenty steps) as
@@ -43,7 +43,10 @@ def _cplx(flat):
     return a[0::2] + 1j * a[1::2]
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    ref_root = ref_root or os.environ.get("S2D_REFERENCE")
+    if not ref_root:
+        raise SystemExit("usage: make_golden.py path/to/reference  (or set S2D_REFERENCE)")
     sp = _load(os.path.join(ref_root, "reference", "spectral2d.py"), "spectral2d")
     fr = _load(os.path.join(ref_root, "reference", "fft_ref.py"), "fft_ref")
     with open(os.path.join(ref_root, "tests", "fixtures.json")) as fh:

@@ -397,6 +397,24 @@ def test_seed_band_statistics(pkg):
         s.destroy()
 
 
+@pytest.mark.parametrize("n,seed", [(256, 0), (1024, 1)])
+def test_seed_band_matches_cpu_restatement(pkg, n, seed):
+    """The benchmark's CPU arms start from wgsl_oracle.band_seed_spectrum: it must be the
+    device seed's field (FP64 Box-Muller rounded to FP32 on both sides; libm and the
+    FP64 sum order may differ in the last FP32 bit)."""
+    from oracle.wgsl_oracle import band_seed_spectrum
+    s = pkg.Solver.create(n=n, dyeScale=1)
+    try:
+        s.seedBand(4.0, 12.0, rms=1.0, seed=seed)
+        got = s.getBuffer("state0")
+        want = band_seed_spectrum(n, 4.0, 12.0, 1.0, seed)
+        assert np.array_equal(got != 0, want != 0)
+        assert rel_l2(got, want) <= 1e-7
+        assert np.max(np.abs(got - want)) <= 2e-7 * np.max(np.abs(want))
+    finally:
+        s.destroy()
+
+
 @pytest.mark.parametrize("graph", [True, False])
 def test_profiler_counts_every_kernel_class(pkg, graph):
     s = pkg.Solver.create(n=128, dyeScale=2)
