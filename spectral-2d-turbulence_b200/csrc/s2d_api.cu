@@ -18,6 +18,7 @@
 #include "s2d_aux_kernels.cuh"
 #include "s2d_ops.cuh"
 #include "s2d_tc.cuh"
+#include "s2d_tc_cols.cuh"
 #include "s2d_render.cuh"
 
 using namespace s2d;
@@ -388,9 +389,9 @@ template <class P> static cudaError_t tc_attrs() {
   chk(cudaFuncSetAttribute(tc::k_fft_tc<0, +1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   chk(cudaFuncSetAttribute(tc::k_fft_tc<1, -1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   chk(cudaFuncSetAttribute(tc::k_fft_tc<1, +1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<0, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
-  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
-  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc<2, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kTcColsSmem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<0, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<2, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
   return e;
 }
 template <class P> static void tc_fft2_launch(float2* buf, int sign, const char* tab, int* err, cudaStream_t st) {
@@ -404,10 +405,10 @@ template <class P> static void tc_fft2_launch(float2* buf, int sign, const char*
   }
 }
 template <class P> static void tc_cols_launch(int mode, const PhysArgs& a, const char* tab, int* err, cudaStream_t st) {
-  const dim3 g(tc::kTcColsGrid), b(tc::kTcThreads);
-  if (mode == 0) tc::k_phys_cols_tc<0, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
-  else if (mode == 1) tc::k_phys_cols_tc<1, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
-  else tc::k_phys_cols_tc<2, P><<<g, b, tc::kTcColsSmem, st>>>(a, tab, err);
+  const dim3 g(tc::kC2Grid), b(tc::kC2Threads);
+  if (mode == 0) tc::k_phys_cols_tc2<0, P><<<g, b, tc::kC2Smem, st>>>(a, tab, err);
+  else if (mode == 1) tc::k_phys_cols_tc2<1, P><<<g, b, tc::kC2Smem, st>>>(a, tab, err);
+  else tc::k_phys_cols_tc2<2, P><<<g, b, tc::kC2Smem, st>>>(a, tab, err);
 }
 static bool is_tc(const s2d_solver* s) { return s->fft_precision != S2D_FFT_FP32; }
 
