@@ -60,6 +60,12 @@ struct GlobalVel {
 __device__ __forceinline__ float lerp1(float a, float b, float t) {
   return __fmaf_rn(b, t, __fmul_rn(a, __fsub_rn(1.f, t)));   // WGSL mix(a, b, t)
 }
+// lerp1 on two channels at once with the packed FP32x2 pipe (sm_100): each lane is the
+// same correctly rounded multiply and fused multiply-add, so the bits equal lerp1's
+__device__ __forceinline__ float2 lerp2v(float2 a, float2 b, float t) {
+  const float omt = __fsub_rn(1.f, t);
+  return __ffma2_rn(b, make_float2(t, t), __fmul2_rn(a, make_float2(omt, omt)));
+}
 
 // bilinear velocity at normalised p (dye.wgsl:27-38); cell indices wrapped
 template <class VF>
@@ -71,8 +77,7 @@ __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, i
   const int ix = (int)bx, iy = (int)by;
   const int x0 = ix & (n - 1), x1 = (ix + 1) & (n - 1), y0 = iy & (n - 1), y1 = (iy + 1) & (n - 1);
   const float2 v00 = vf(x0, y0), v10 = vf(x1, y0), v01 = vf(x0, y1), v11 = vf(x1, y1);
-  return make_float2(lerp1(lerp1(v00.x, v10.x, fx), lerp1(v01.x, v11.x, fx), fy),
-                     lerp1(lerp1(v00.y, v10.y, fx), lerp1(v01.y, v11.y, fx), fy));
+  return lerp2v(lerp2v(v00, v10, fx), lerp2v(v01, v11, fx), fy);
 }
 
 __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - d + 1)
@@ -82,13 +87,20 @@ __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - 
 
 // midpoint back-trace (dye.wgsl:40-45), from the velocity v1 already sampled at p
 // (0.5 (v h) is v (h/2): halving commutes with the rounding of the product)
+// fract(p - v s + 1) on both coordinates with the packed pipe (same bits as fract_shift:
+// p - d is p + (-d), and the negation is exact)
+__device__ __forceinline__ float2 fract_shift2(float2 p, float2 v, float s) {
+  const float2 d = __fmul2_rn(v, make_float2(-s, -s));
+  const float2 x = __fadd2_rn(__fadd2_rn(p, d), make_float2(1.f, 1.f));
+  return make_float2(__fsub_rn(x.x, floorf(x.x)), __fsub_rn(x.y, floorf(x.y)));
+}
 template <class VF>
 __device__ __forceinline__ float2 trace_from(const VF& vf, float px, float py, float2 v1, float h, int n) {
   const float hh = 0.5f * h;
-  const float mx = fract_shift(px, __fmul_rn(v1.x, hh));
-  const float my = fract_shift(py, __fmul_rn(v1.y, hh));
-  const float2 v2 = sample_vel(vf, mx, my, n);
-  return make_float2(fract_shift(px, __fmul_rn(v2.x, h)), fract_shift(py, __fmul_rn(v2.y, h)));
+  const float2 p = make_float2(px, py);
+  const float2 mid = fract_shift2(p, v1, hh);
+  const float2 v2 = sample_vel(vf, mid.x, mid.y, n);
+  return fract_shift2(p, v2, h);
 }
 template <class VF>
 __device__ __forceinline__ float2 trace_pos(const VF& vf, float px, float py, float h, int n) {
@@ -129,8 +141,11 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
     hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
     hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
   }
-  return {lerp2(c00.r, c10.r, c01.r, c11.r, f.fx, f.fy), lerp2(c00.g, c10.g, c01.g, c11.g, f.fx, f.fy),
-          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy), lerp2(c00.a, c10.a, c01.a, c11.a, f.fx, f.fy)};
+  const float2 rg = lerp2v(lerp2v(make_float2(c00.r, c00.g), make_float2(c10.r, c10.g), f.fx),
+                           lerp2v(make_float2(c01.r, c01.g), make_float2(c11.r, c11.g), f.fx), f.fy);
+  const float2 ba = lerp2v(lerp2v(make_float2(c00.b, c00.a), make_float2(c10.b, c10.a), f.fx),
+                           lerp2v(make_float2(c01.b, c01.a), make_float2(c11.b, c11.a), f.fx), f.fy);
+  return {rg.x, rg.y, ba.x, ba.y};
 }
 
 // texel centre (x + 0.5)/m; m is a power of two, so x/m, 0.5/m and their sum (2x+1)/(2m)
@@ -314,8 +329,7 @@ __device__ __forceinline__ float2 sample_vel_win(const SmemVel& vf, float px, fl
     v01 = vf(x0, y1);
     v11 = vf(x1, y1);
   }
-  return make_float2(lerp1(lerp1(v00.x, v10.x, fx), lerp1(v01.x, v11.x, fx), fy),
-                     lerp1(lerp1(v00.y, v10.y, fx), lerp1(v01.y, v11.y, fx), fy));
+  return lerp2v(lerp2v(v00, v10, fx), lerp2v(v01, v11, fx), fy);
 }
 struct WinVel {      // adapter: the window sampler where trace_from expects sample_vel
   const SmemVel& v;
@@ -344,8 +358,9 @@ __device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb*
     hi->g = fmaxf(fmaxf(c00.g, c10.g), fmaxf(c01.g, c11.g));
     hi->b = fmaxf(fmaxf(c00.b, c10.b), fmaxf(c01.b, c11.b));
   }
-  return {lerp2(c00.r, c10.r, c01.r, c11.r, f.fx, f.fy), lerp2(c00.g, c10.g, c01.g, c11.g, f.fx, f.fy),
-          lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy)};
+  const float2 rg = lerp2v(lerp2v(make_float2(c00.r, c00.g), make_float2(c10.r, c10.g), f.fx),
+                           lerp2v(make_float2(c01.r, c01.g), make_float2(c11.r, c11.g), f.fx), f.fy);
+  return {rg.x, rg.y, lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy)};
 }
 
 // binary16 W x WY window whose texels outside the window are re-derived by EVAL
