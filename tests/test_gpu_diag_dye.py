@@ -97,8 +97,10 @@ def test_paint_bands(pkg, m_scale):
         s.reset({"k0": 14, "amplitude": 6, "seed": 1, "dyePattern": "bands"})
         got = s.currentDye
         want = wo.paint_dye_bands(n * m_scale)
+        # toHalf (solver.js:20-41) is integer work on the FP32 rounding of the same double
+        # expression: bit for bit
         diff = np.abs(got.astype(np.int32) - want.astype(np.int32))
-        assert diff.max() <= 1 and np.mean(diff != 0) < 1e-3
+        assert np.count_nonzero(diff) == 0, f"{np.count_nonzero(diff)} texel channels differ, max {diff.max()}"
     finally:
         s.destroy()
 

@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 def _instances():
     rng = np.random.default_rng(42)
     out = []
-    for n, count in ((64, 3), (128, 2), (256, 2), (512, 1)):
+    for n, count in ((64, 3), (128, 2), (256, 2), (512, 1), (1024, 1)):   # every accepted size, 64..1024
         for _ in range(count):
             out.append({"n": n, "beta": float(rng.uniform(0, 20)), "drag": float(rng.uniform(0, 2e-2)),
                         "nuH": float(rng.uniform(1e-4, 1e-3)), "hyperP": 1, "dt": 2e-3,

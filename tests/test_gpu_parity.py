@@ -466,7 +466,8 @@ def test_tc_precision_only_at_1024(pkg):
 def test_precision_sweep_fft_and_step(pkg):
     """FP32, FP16-split and BF16-split FFT paths at 1024^2 against FP64: 2D FFT and one
     fused step (rel L2, printed).  FP32 and the FP16 split meet 1e-5; the BF16 split keeps
-    16 significant bits per operand (the FP16 split 22), so its error is larger."""
+    16 significant bits per operand (the FP16 split 22), so its error is larger but still
+    under the 1e-5 bar."""
     n, dt = 1024, 1e-3
     rng = np.random.default_rng(3)
     a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
@@ -496,7 +497,9 @@ def test_precision_sweep_fft_and_step(pkg):
         print(f"{fft}: 2D FFT rel L2 {e_fft:.3e}, one step rel L2 {e_step:.3e}")
     assert errs["fp32"][0] <= 1e-5 and errs["fp32"][1] <= 1e-5
     assert errs["tc-f16"][0] <= 1e-5 and errs["tc-f16"][1] <= 1e-5
-    assert errs["tc-bf16"][0] <= 1e-3 and errs["tc-bf16"][1] <= 1e-3
+    # the BF16 split keeps 16 significant bits per operand (6.5e-6 / 2.5e-6 measured): it
+    # meets the same 1e-5 bar with less margin than the FP16 split
+    assert errs["tc-bf16"][0] <= 1e-5 and errs["tc-bf16"][1] <= 1e-5
     assert errs["tc-bf16"][0] > errs["tc-f16"][0]
 
 
