@@ -187,8 +187,10 @@ int s2d_reset_scenario(s2d_solver* s, int kind, double param, int dye_pattern);
  * state saved and restored around every trial), keeps the fastest column shape and
  * then the fastest row shape with it, drops captured step graphs, and remembers the
  * choice for later solvers of the same size, FFT precision and device.  Results
- * differ from the default shape by FP32 rounding only. */
-#define S2D_TUNE_MAX 4
+ * differ from the default shape by FP32 rounding only.  A tensor-core solver has one
+ * row shape more, the last index: the row stage as split-precision DFT-GEMMs on the
+ * tensor cores (its transforms then round like the column stage's). */
+#define S2D_TUNE_MAX 8
 typedef struct {
   int32_t phys_variants, spec_variants;   /* registered column / row shapes */
   int32_t phys_choice, spec_choice;       /* the shapes now in use */

@@ -57,7 +57,7 @@ class s2d_splat(C.Structure):
                 ("dye_amp", C.c_float)]
 
 
-S2D_TUNE_MAX = 4
+S2D_TUNE_MAX = 8
 
 
 class s2d_tune_report(C.Structure):

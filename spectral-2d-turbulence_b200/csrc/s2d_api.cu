@@ -193,6 +193,13 @@ struct s2d_solver {
   int prof_cnt[S2D_PROF_CLASSES] = {0};
 };
 
+// Row-stage variants of a solver: the registered FP32 shapes, plus (last index) the row
+// stage on the tensor cores for a tensor-core solver.
+static int spec_variants(const s2d_solver* s) { return s->ops->n_spec + (s->fft_precision != S2D_FFT_FP32 ? 1 : 0); }
+static bool tc_rows(const s2d_solver* s) {
+  return s->fft_precision != S2D_FFT_FP32 && s->spec_choice == s->ops->n_spec;
+}
+
 // Stage-kernel shapes chosen by s2d_autotune, per (device, n, FFT precision), shared by
 // the solvers created afterwards in this process.
 static std::mutex g_tune_mu;
@@ -202,7 +209,7 @@ static void tuned_choice(s2d_solver* s) {
   auto it = g_tuned.find(std::make_tuple(s->dev, s->n, s->fft_precision));
   if (it == g_tuned.end()) return;
   if (it->second.first < s->ops->n_phys) s->phys_choice = it->second.first;
-  if (it->second.second < s->ops->n_spec) s->spec_choice = it->second.second;
+  if (it->second.second < spec_variants(s)) s->spec_choice = it->second.second;
 }
 static void remember_choice(s2d_solver* s) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -392,6 +399,13 @@ template <class P> static cudaError_t tc_attrs() {
   chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<0, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
   chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<1, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
   chk(cudaFuncSetAttribute(tc::k_phys_cols_tc2<2, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<-1, false, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<0, false, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<1, false, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<2, false, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<0, true, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<1, true, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
+  chk(cudaFuncSetAttribute(tc::k_spec_rows_tc2<2, true, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kC2Smem));
   return e;
 }
 template <class P> static void tc_fft2_launch(float2* buf, int sign, const char* tab, int* err, cudaStream_t st) {
@@ -410,7 +424,31 @@ template <class P> static void tc_cols_launch(int mode, const PhysArgs& a, const
   else if (mode == 1) tc::k_phys_cols_tc2<1, P><<<g, b, tc::kC2Smem, st>>>(a, tab, err);
   else tc::k_phys_cols_tc2<2, P><<<g, b, tc::kC2Smem, st>>>(a, tab, err);
 }
+// the row stage on the tensor cores: mode -1 = prime (pack wcur only), 0..2 = RK stage
+template <class P> static void tc_rows_launch(int mode, bool ptr, const SpecArgs& a, const char* tab, cudaStream_t st) {
+  const dim3 g(512 / tc::kC2Wg), b(tc::kC2Threads);
+  const int sm = tc::kC2Smem;
+  if (mode < 0) tc::k_spec_rows_tc2<-1, false, P><<<g, b, sm, st>>>(a, tab);
+  else if (!ptr) {
+    if (mode == 0) tc::k_spec_rows_tc2<0, false, P><<<g, b, sm, st>>>(a, tab);
+    else if (mode == 1) tc::k_spec_rows_tc2<1, false, P><<<g, b, sm, st>>>(a, tab);
+    else tc::k_spec_rows_tc2<2, false, P><<<g, b, sm, st>>>(a, tab);
+  } else {
+    if (mode == 0) tc::k_spec_rows_tc2<0, true, P><<<g, b, sm, st>>>(a, tab);
+    else if (mode == 1) tc::k_spec_rows_tc2<1, true, P><<<g, b, sm, st>>>(a, tab);
+    else tc::k_spec_rows_tc2<2, true, P><<<g, b, sm, st>>>(a, tab);
+  }
+}
 static bool is_tc(const s2d_solver* s) { return s->fft_precision != S2D_FFT_FP32; }
+// the row stage with the solver's chosen variant
+static void run_spec(s2d_solver* s, int mode, bool ptr, const SpecArgs& a) {
+  if (tc_rows(s)) {
+    if (s->fft_precision == S2D_FFT_TC_BF16) tc_rows_launch<tc::PrecBF16>(mode, ptr, a, s->tctab, s->stream);
+    else tc_rows_launch<tc::PrecF16>(mode, ptr, a, s->tctab, s->stream);
+  } else {
+    s->ops->spec[s->spec_choice].run(mode, ptr, a, s->stream);
+  }
+}
 
 extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s2d_solver** out) {
   if (!out) return fail(S2D_ERR_ARG, "out is null");
@@ -692,7 +730,7 @@ static int enqueue_pack_prime(s2d_solver* s) {
   a.tw = s->tw;
   a.err = s->err;
   a.row_nz = s->row_nz;
-  s->ops->spec[s->spec_choice].run(-1, false, a, s->stream);
+  run_spec(s, -1, false, a);
   S2D_LAUNCHED();
   s->packs_flagged = true;
   s->packs_valid = true;
@@ -791,7 +829,7 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     a.stochastic = s->hp.force_amp > 0.f ? 1 : 0;
     a.err = s->err;
     a.row_nz = s->row_nz;
-    s->ops->spec[s->spec_choice].run(st, ptr, a, s->stream);
+    run_spec(s, st, ptr, a);
     S2D_LAUNCHED();
     s->packs_flagged = true;
   }
@@ -1185,16 +1223,19 @@ static void drop_graphs(s2d_solver* s) {
 extern "C" int s2d_tune_variant_name(s2d_solver* s, int kind, int index, char* out, int cap) {
   S2D_USE(s);
   if (!out || cap <= 0) return fail(S2D_ERR_ARG, "output is null");
-  const int count = kind == 0 ? s->ops->n_phys : kind == 1 ? s->ops->n_spec : -1;
+  const int count = kind == 0 ? s->ops->n_phys : kind == 1 ? spec_variants(s) : -1;
   if (count < 0) return fail(S2D_ERR_ARG, "kind is 0 (column) or 1 (row)");
   if (index < 0 || index >= count) return fail(S2D_ERR_ARG, "variant index out of range");
-  std::snprintf(out, (size_t)cap, "%s", kind == 0 ? s->ops->phys[index].name : s->ops->spec[index].name);
+  const char* name = kind == 0 ? s->ops->phys[index].name
+                     : index == s->ops->n_spec ? "tensor-core rows (split DFT-GEMM x-transforms)"
+                                               : s->ops->spec[index].name;
+  std::snprintf(out, (size_t)cap, "%s", name);
   return S2D_OK;
 }
 
 extern "C" int s2d_tune_select(s2d_solver* s, int phys, int spec) {
   S2D_USE(s);
-  if (phys < 0 || phys >= s->ops->n_phys || spec < 0 || spec >= s->ops->n_spec)
+  if (phys < 0 || phys >= s->ops->n_phys || spec < 0 || spec >= spec_variants(s))
     return fail(S2D_ERR_ARG, "variant index out of range");
   DeviceGuard guard(s->dev);
   s->phys_choice = phys;
@@ -1259,7 +1300,7 @@ extern "C" int s2d_autotune(s2d_solver* s, int steps, s2d_tune_report* report) {
   };
   s2d_tune_report rep{};
   rep.phys_variants = s->ops->n_phys;
-  rep.spec_variants = s->ops->n_spec;
+  rep.spec_variants = spec_variants(s);
   const int p0 = s->phys_choice, q0 = s->spec_choice;
   // the tensor-core column stage has one shape: only the row shapes are tuned there
   const bool tc = is_tc(s);
@@ -1274,7 +1315,7 @@ extern "C" int s2d_autotune(s2d_solver* s, int steps, s2d_tune_report* report) {
     }
     s->phys_choice = best_p;
     best = 1e30f;
-    for (int j = 0; j < s->ops->n_spec && !rc; ++j) {
+    for (int j = 0; j < spec_variants(s) && !rc; ++j) {
       s->spec_choice = j;
       rc = trial(&rep.spec_us[j]);
       if (!rc && rep.spec_us[j] < best) { best = rep.spec_us[j]; best_q = j; }

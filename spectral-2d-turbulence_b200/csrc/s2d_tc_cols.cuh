@@ -342,3 +342,259 @@ done:
 
 }  // namespace tc
 }  // namespace s2d
+
+namespace s2d {
+namespace tc {
+
+// ---------------------------------------------------------------------------------------
+// The spectral-row stage at 1024^2 on the tensor cores (the tcgen05 counterpart of
+// k_spec_rows), in the same warpgroup-chain form: a CTA runs two WGs, WG g owns the row
+// pair p = 2 blockIdx.x + g (rows p and N - p; pair 0 is rows 0 and N/2).
+//   forward x-transform of the two Z rows (rows 0..63 of an M = 128 block, line-major:
+//     row = line * 32 + n1, so a warp's loads are consecutive in x)
+//   Z_hat staged in natural order in the WG's operand buffer; all 128 threads then unpack
+//     (partner row, Hermitian), form N_hat with the 2/3 mask, add forcing, apply the
+//     integrating-factor RK3 stage update and form the next packs: thread (row line,
+//     n1 = lane, n2 half) holds the cells kx = n1 + 32 n2 -- exactly its part of the
+//     inverse transform's step-A operand rows, so no transposition is needed
+//   inverse x-transform of the 4 pack lines (PA, PB of both rows; one M = 128 block),
+//     written to PA / PB rows with lane-consecutive x
+// The WG-wide power-of-two scale of the packs is read after the barrier that also
+// decides whether both rows are all zero (then the inverse and its stores are skipped
+// and the rows flagged, as the FP32 kernel does).
+template <int MODE, bool PTR, class P = PrecF16>
+__global__ void __launch_bounds__(kC2Threads, 2) k_spec_rows_tc2(SpecArgs a, const char* __restrict__ tab) {
+  constexpr int N = 1024;
+  constexpr float KCUT = Tune<N>::KCUT;
+  extern __shared__ __align__(1024) char sm[];
+  char* misc = sm + kC2OffMisc;
+  uint64_t* setup = reinterpret_cast<uint64_t*>(misc + kC2MiscSetup);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(misc + kC2MiscTmem);
+  float* wmax = reinterpret_cast<float*>(misc + kC2MiscMax);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wg = tid >> 7, wt = tid & 127, wq = warp & 3;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(misc + kC2MiscBar) + wg;
+  int* s_nz = reinterpret_cast<int*>(misc + kC2MiscRowScale) + 8 * wg;   // per-warp "row holds a nonzero"
+  char* op = sm + kC2OffOp + wg * kC2Op;
+  float2* zs = reinterpret_cast<float2*>(op);                             // Z_hat staging [2][N]
+  const uint32_t op_s = smem_u32(op), b_s = smem_u32(sm + kC2OffB);
+  int* err = a.err;
+  const int pair = blockIdx.x * kC2Wg + wg;
+  const int row0 = pair == 0 ? 0 : pair, row1 = pair == 0 ? N / 2 : N - pair;
+  auto row_of_line = [&](int l) { return l ? row1 : row0; };   // selects, not an indexed array
+
+  if (warp == 0) {
+    tmem_alloc(tslot, 64 * kC2Wg);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(setup, 1);
+    for (int g = 0; g < kC2Wg; ++g) mbar_init(reinterpret_cast<uint64_t*>(misc + kC2MiscBar) + g, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(setup, 2 * kBBytes + kTcTwBytes);
+    bulk_g2s(sm + kC2OffB, tab + kTabFwd, 2 * kBBytes + kTcTwBytes, setup);
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = *tslot + 64u * wg;
+  const uint32_t trow_addr = tmem + ((uint32_t)(32 * wq) << 16);
+
+  bool bad = false, abort = false;
+  uint32_t phase = 0, issued = 2u;
+  // the first pair has the smallest |ky|: the WG is uniformly in or out of band work
+  const bool any_band = MODE >= 0 && (float)pair < KCUT;
+  // this thread's cells: row line `ln`, x = n1 + 32 n2 for n2 in [16 h, 16 h + 16)
+  const int ln = wq & 1, n1 = lane, h = wq >> 1;
+  const int row = row_of_line(ln);
+  const float ky = wn<N>(row);
+  const bool row_band = fabsf(ky) < KCUT;
+  float2 nhat[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) nhat[j] = make_float2(0.f, 0.f);
+
+  if (any_band) {
+    // ---- forward x-transform of the two Z rows: step-A row wt = (line, n1), wt < 64
+    float mx = 0.f, sA = 1.f;
+    if (wt < 64) {
+      const int zl = wt >> 5;
+      const int zrow = row_of_line(zl);
+      const bool zb = fabsf(wn<N>(zrow)) < KCUT;
+      float2 v[32];
+#pragma unroll
+      for (int n2 = 0; n2 < 32; ++n2)
+        v[n2] = zb ? __ldcs(a.z + (size_t)zrow * N + lane + 32 * n2) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int n2 = 0; n2 < 32; ++n2) mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
+      sA = pow2_scale(mx);
+#pragma unroll
+      for (int kc = 0; kc < 8; ++kc) c2_put4<P>(op, wt, kc, &v[4 * kc], sA, sA);
+    }
+    mx = warp_max(mx);
+    if (lane == 0) wmax[warp] = mx;
+    if (wt == 0) bad |= !mbar_wait_bounded(setup, 0u, err, 4);
+    abort = c2_issue<P>(wg, wt, bad, tmem, op_s, b_s, bar);
+    if (abort) goto done;
+    issued = phase;
+    {
+      const float mall = fmaxf(wmax[4 * wg], wmax[4 * wg + 1]);
+      const float sC = pow2_scale(mall) * 0.03125f;
+      float y[64];
+      if (wt < 64) {
+        bad |= !mbar_wait_bounded(setup, 0u, err, 4);
+        bad |= !mbar_wait_bounded(bar, phase, err, 2);
+        fence_after_sync();
+        c2_tmem_read64(trow_addr, y);
+        const int zl = wt >> 5;
+        c2_twiddle_scatter<P>(y, sm, op, lane, sC / sA, [&](int k2) { return 32 * zl + k2; });
+      }
+      phase ^= 1u;
+      abort = c2_issue<P>(wg, wt, bad, tmem, op_s, b_s, bar);
+      if (abort) goto done;
+      issued = phase;
+      if (wt < 64) {
+        // step C done: row wt = (line, k2), X[k2 + 32 k1] into the natural-order staging
+        bad |= !mbar_wait_bounded(bar, phase, err, 3);
+        fence_after_sync();
+        c2_tmem_read64(trow_addr, y);
+        const int zl = wt >> 5;
+        const float inv = 1.f / sC;
+#pragma unroll
+        for (int k1 = 0; k1 < 32; ++k1) zs[zl * N + lane + 32 * k1] = make_float2(y[2 * k1] * inv, y[2 * k1 + 1] * inv);
+      }
+      phase ^= 1u;
+    }
+    if (wg_bar_or(wg, bad)) goto done;   // staging visible to the WG
+    {
+      // ---- Hermitian unpack through the partner row, N_hat = i kx q1 + i ky q2, 2/3 mask
+      const int pln = pair == 0 ? ln : ln ^ 1;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = n1 + 32 * (16 * h + j);
+        const float kx = wn<N>(c);
+        const float2 zk = zs[ln * N + c];
+        const float2 zm = cconj(zs[pln * N + ((N - c) & (N - 1))]);
+        const float2 q1 = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+        const float2 dd = csub(zk, zm);
+        const float2 q2 = make_float2(0.5f * dd.y, -0.5f * dd.x);
+        const bool band = row_band && fabsf(kx) < KCUT;
+        nhat[j] = band ? make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x) : make_float2(0.f, 0.f);
+      }
+    }
+    wg_bar_or(wg, false);                // staging reads done before the operand rewrites it
+  }
+  {
+    // ---- RK3 stage update of this thread's 16 cells (solver.wgsl:97-122), next packs
+    const DevParams& Pp = *a.params;
+    float dt = 0.f;
+    if constexpr (MODE >= 0) dt = __ldg(a.dt);
+    const float2 fb2 = forcing_k2_bounds(Pp);
+    constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+    const size_t rbase = (size_t)row * N;
+    float2 pa[16], pb[16];
+    float mp = 0.f;
+    bool nzr = false;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int c = n1 + 32 * (16 * h + j);
+      const float kx = wn<N>(c);
+      const float k2 = kx * kx + ky * ky;
+      const float2 wc = a.wcur[rbase + c];
+      float2 w;
+      if constexpr (MODE < 0) {
+        w = wc;
+      } else {
+        const float2 w0 = MODE == 0 ? wc : a.w0[rbase + c];
+        const bool band = row_band && fabsf(kx) < KCUT;
+        float2 rhs = make_float2(-nhat[j].x, -nhat[j].y);
+        if constexpr (PTR) {
+          if (band) rhs = cadd(rhs, __ldg(a.fptr + rbase + c));
+        }
+        if (a.stochastic && band && k2 > 0.f && k2 >= fb2.x && k2 <= fb2.y)
+          rhs = cadd(rhs, stochastic_term(Pp, N, row, c, kx, ky, k2, dt));
+        const bool quiet = wc.x == 0.f && wc.y == 0.f && w0.x == 0.f && w0.y == 0.f && rhs.x == 0.f && rhs.y == 0.f;
+        if (k2 == 0.f || quiet) w = make_float2(0.f, 0.f);
+        else w = rk_update<MODE>(half_factor_m1(Pp, kx, k2, dt), w0, wc, rhs, dt);
+        a.wout[rbase + c] = w;
+      }
+      nzr |= (w.x != 0.f || w.y != 0.f);
+      const float inv = k2 > 0.f ? __frcp_rn(k2) : 0.f;
+      const float fa = (1.f - ky * inv) * inv_n2;     // w + i u_hat = w (1 - ky/k2)
+      const float fbk = kx * inv * inv_n2;            // v_hat = -i kx w / k2
+      pa[j] = make_float2(w.x * fa, w.y * fa);
+      pb[j] = make_float2(w.y * fbk, -w.x * fbk);
+      mp = fmaxf(mp, fmaxf(fmaxf(fabsf(pa[j].x), fabsf(pa[j].y)), fmaxf(fabsf(pb[j].x), fabsf(pb[j].y))));
+    }
+    mp = warp_max(mp);
+    const int wnz = __any_sync(0xffffffffu, nzr) ? 1 : 0;
+    const int wbad = __any_sync(0xffffffffu, bad) ? 1 : 0;
+    if (lane == 0) {
+      wmax[warp] = mp;
+      s_nz[wq] = wnz;
+      s_nz[4 + wq] = wbad;
+    }
+    wg_bar_or(wg, false);
+    // every thread reads the same words after the barrier: the decisions below are uniform
+    const int nz0 = s_nz[0] | s_nz[2], nz1 = s_nz[1] | s_nz[3];
+    const bool any_bad = (s_nz[4] | s_nz[5] | s_nz[6] | s_nz[7]) != 0;
+    if (a.row_nz && wt == 0) {
+      a.row_nz[row0] = nz0;
+      a.row_nz[row1] = nz1;
+    }
+    if (any_bad) goto done;
+    if (a.row_nz && !(nz0 | nz1)) goto done;   // both rows zero: no transforms, no stores (flagged)
+    // ---- inverse x-transforms: step-A rows (line' = 2 ln + {PA, PB}) * 32 + n1, K chunks 4h..4h+3,
+    // input conjugated (the inverse as conj(F(conj x)))
+    const float mall = fmaxf(fmaxf(wmax[4 * wg], wmax[4 * wg + 1]), fmaxf(wmax[4 * wg + 2], wmax[4 * wg + 3]));
+    const float sA = pow2_scale(mall);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      c2_put4<P>(op, (2 * ln) * 32 + n1, 4 * h + q, &pa[4 * q], sA, -sA);
+      c2_put4<P>(op, (2 * ln + 1) * 32 + n1, 4 * h + q, &pb[4 * q], sA, -sA);
+    }
+    if (!any_band && wt == 0) bad |= !mbar_wait_bounded(setup, 0u, err, 4);   // first GEMM of this WG
+    abort = c2_issue<P>(wg, wt, bad, tmem, op_s, b_s, bar);
+    if (abort) goto done;
+    issued = phase;
+    const float sC = sA * 0.03125f;
+    float y[64];
+    bad |= !mbar_wait_bounded(setup, 0u, err, 4);
+    bad |= !mbar_wait_bounded(bar, phase, err, 2);
+    phase ^= 1u;
+    fence_after_sync();
+    c2_tmem_read64(trow_addr, y);
+    {
+      const int lp = wt >> 5;   // line' of this thread's step-A row (row wt = line' * 32 + n1)
+      c2_twiddle_scatter<P>(y, sm, op, lane, 0.03125f, [&](int k2) { return 32 * lp + k2; });
+    }
+    abort = c2_issue<P>(wg, wt, bad, tmem, op_s, b_s, bar);
+    if (abort) goto done;
+    issued = phase;
+    bad |= !mbar_wait_bounded(bar, phase, err, 3);
+    phase ^= 1u;
+    fence_after_sync();
+    c2_tmem_read64(trow_addr, y);
+    {
+      // row wt = (line' = wt / 32, k2 = lane): conj(D) / sC at x = k2 + 32 k1
+      const int lp = wt >> 5;
+      float2* dst = ((lp & 1) ? a.pb : a.pa) + (size_t)row_of_line(lp >> 1) * N + lane;
+      const float inv = 1.f / sC;
+#pragma unroll
+      for (int k1 = 0; k1 < 32; ++k1) dst[32 * k1] = make_float2(y[2 * k1] * inv, -y[2 * k1 + 1] * inv);
+    }
+  }
+done:
+  if (__syncthreads_or(bad ? 1 : 0)) {
+    if (tid == 0) mbar_wait_bounded(setup, 0u, nullptr, 0);
+    if (wt == 0 && issued < 2u) mbar_wait_bounded(bar, issued, nullptr, 0);
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    tmem_dealloc(*tslot, 64 * kC2Wg);
+  }
+}
+
+}  // namespace tc
+}  // namespace s2d

@@ -283,6 +283,17 @@ class Solver:
         return {"column": col, "row": row,
                 "choice": {"column": col[rep.phys_choice][0], "row": row[rep.spec_choice][0]}}
 
+    def tuneVariantNames(self, kind: str = "row") -> list:
+        """Names of the registered launch shapes of the column ("column") or row ("row")
+        stage; for a tensor-core solver the last row shape is the row stage on the
+        tensor cores."""
+        k = 0 if kind == "column" else 1
+        names = []
+        buf = C.create_string_buffer(64)
+        while L.lib().s2d_tune_variant_name(self._use(), k, len(names), buf, 64) == 0:
+            names.append(buf.value.decode())
+        return names
+
     def tuneSelect(self, column: int, row: int):
         """Use registered stage-kernel shapes `column` / `row` (indices of autotune's lists)."""
         L.call("s2d_tune_select", self._use(), int(column), int(row))

@@ -62,9 +62,12 @@ def _report(name, fft, err):
     print(f"\n[long-run] {name} fft={fft} " + " ".join(f"{k}={v:.3e}" for k, v in err.items()))
 
 
-def _run_fixed(s, steps, chunk=250):
-    """`steps` fused RK3 steps at the fixed dt already in the dt slot (no CFL, no dye),
-    each substep with its own forcing phase (stepIndex 0, 1, 2, ...)."""
+def _run_fixed(s, steps, dt, chunk=250):
+    """`steps` fused RK3 steps at the fixed `dt` (no CFL, no dye), each substep with its own
+    forcing phase (stepIndex 0, 1, 2, ...).  The solver is primed first: priming runs the
+    CFL reduction, so the fixed dt is written after it."""
+    s.encodePrime()
+    set_fixed_dt(s, dt)
     done = 0
     while done < steps:
         k = min(chunk, steps - done)
@@ -115,8 +118,7 @@ def test_config1_free_decay_256(pkg, fft):
         s.seedBand(6.0, 10.0, rms=1.0, seed=0)
         w0 = current_state(s)
         nu_h = float(s.paramsF[2])
-        set_fixed_dt(s, dt)
-        _run_fixed(s, steps)
+        _run_fixed(s, steps, dt)
         got = current_state(s)
     finally:
         s.destroy()
@@ -153,8 +155,7 @@ def test_config4_beta_plane_4096(pkg, fft):
         s.configure(cfg)
         load_state(s, np.zeros((n, n), np.complex64))
         nu_h = float(s.paramsF[2])
-        set_fixed_dt(s, dt)
-        _run_fixed(s, steps)
+        _run_fixed(s, steps, dt)
         got = current_state(s)
     finally:
         s.destroy()
@@ -182,8 +183,7 @@ def _taylor_green(pkg, n, steps, fft, jac_bound, rate_bound, nu=1e-3, dt=2e-3):
         s.seedPhysical(6.0 * np.cos(2 * gx) * np.cos(2 * gy))
         w0 = current_state(s).astype(np.complex128)
         nu_h = float(s.paramsF[2])
-        set_fixed_dt(s, dt)
-        _run_fixed(s, steps)
+        _run_fixed(s, steps, dt)
         w1 = current_state(s).astype(np.complex128)
     finally:
         s.destroy()
@@ -208,8 +208,7 @@ def _compare_run(pkg, name, n, fft, field, nu, dt, steps, bounds):
         s.seedPhysical(field)
         w0 = current_state(s)
         nu_h = float(s.paramsF[2])
-        set_fixed_dt(s, dt)
-        _run_fixed(s, steps)
+        _run_fixed(s, steps, dt)
         got = current_state(s)
     finally:
         s.destroy()

@@ -503,8 +503,17 @@ def test_precision_sweep_fft_and_step(pkg):
     assert errs["tc-bf16"][0] > errs["tc-f16"][0]
 
 
-def _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt):
+def _tc_rows(s):
+    """Pin the row stage of tensor-core solver `s` to the tensor-core row kernel."""
+    names = s.tuneVariantNames("row")
+    assert names[-1].startswith("tensor-core rows")
+    s.tuneSelect(0, len(names) - 1)
+
+
+def _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt, rows="fp32"):
     s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+    if rows == "tc":
+        _tc_rows(s)
     s.configure(config(beta=beta, drag=mu, viscosity=rate_for(nu_h, n, p), hyperP=p))
     load_state(s, w_in)
     set_fixed_dt(s, dt)
@@ -512,17 +521,20 @@ def _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt):
     return s
 
 
+@pytest.mark.parametrize("rows", ["fp32", "tc"])
+@pytest.mark.parametrize("fft", ["tc-f16", "tc-bf16"])
 @pytest.mark.parametrize("beta", [0.0, 10.0])
-def test_tc_fused_step_vs_oracle(pkg, beta):
-    """Fused RK3 step with the tensor-core column stage (split FP16 DFT-GEMMs) vs the
-    FP64 oracle at 1024^2: rel L2 <= 1e-5 after one step, <= 3e-5 after five."""
+def test_tc_fused_step_vs_oracle(pkg, beta, fft, rows):
+    """Fused RK3 step with the tensor-core column stage (split FP16 / BF16 DFT-GEMMs),
+    with the FP32 or the tensor-core row stage, vs the FP64 oracle at 1024^2: rel L2
+    <= 1e-5 after one step, <= 3e-5 after five."""
     n, mu, p, dt, amp = 1024, 1e-2, 4, 1e-3, 8.0
     nu_h = 1.0 / (n / 3.0) ** 8
     ref = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
     ref.set_vorticity(random_field(n, k0=n / 8, seed=11, amplitude=amp))
     w_in = ref.w.astype(np.complex64)
     ref.w = w_in.astype(np.complex128)
-    s = _tc_case_solver(pkg, "tc-f16", n, beta, mu, nu_h, p, w_in, dt)
+    s = _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt, rows=rows)
     try:
         s.encodeStep()
         ref.step(dt=dt)
@@ -531,7 +543,7 @@ def test_tc_fused_step_vs_oracle(pkg, beta):
             s.encodeStep()
             ref.step(dt=dt)
         err5 = rel_l2(current_state(s), ref.w)
-        print(f"tc fused step rel L2: 1 step {err1:.3e}, 5 steps {err5:.3e}")
+        print(f"{fft} rows={rows} fused step rel L2: 1 step {err1:.3e}, 5 steps {err5:.3e}")
         assert err1 <= 1e-5, f"one step rel L2 {err1:.3e}"
         assert err5 <= 3e-5, f"five steps rel L2 {err5:.3e}"
     finally:
@@ -567,24 +579,30 @@ def test_tc_forced_run_tracks_fp32(pkg):
     n = 1024
     w = random_field(n, k0=14, seed=1, amplitude=6.0)
     out = {}
-    for fft in ("fp32", "tc-f16"):
-        s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+    for key in ("fp32", "tc-f16", "tc-f16+rows"):
+        s = pkg.Solver.create(n=n, dyeScale=1, fft=key.split("+")[0])
         try:
+            if key.endswith("+rows"):
+                _tc_rows(s)
             s.configure(config(viscosity=1.0, hyperP=4, drag=1e-2, forceAmp=0.1, forceK=64.0, forceWidth=2.0,
                                cfl=0.5, dtMax=1e-3))
             s.reset({"field": w, "dyePattern": "bands"})
+            s.setSplats([{"x": 0.3, "y": 0.6, "dx": 2.0, "dy": -1.0, "color": [1.0, 0.5, 0.2], "radius": 0.03,
+                          "amp": 1.0, "dyeAmp": 1.0}])
             s.step(5, dye=True, reduce=True, graph=True)
-            out[fft] = (current_state(s), s.getBuffer("dt"), s.getBuffer("vel"))
+            out[key] = (current_state(s), s.getBuffer("dt"), s.getBuffer("vel"))
         finally:
             s.destroy()
-    e_state = rel_l2(out["tc-f16"][0], out["fp32"][0])
-    e_vel = rel_l2(out["tc-f16"][2], out["fp32"][2])
-    print(f"tc vs fp32 after 5 forced steps: state {e_state:.3e} vel {e_vel:.3e}")
-    assert e_state <= 1e-5 and e_vel <= 1e-5
-    assert abs(float(out["tc-f16"][1][0]) / float(out["fp32"][1][0]) - 1) <= 1e-5
+    for key in ("tc-f16", "tc-f16+rows"):
+        e_state = rel_l2(out[key][0], out["fp32"][0])
+        e_vel = rel_l2(out[key][2], out["fp32"][2])
+        print(f"{key} vs fp32 after 5 forced steps (stochastic + pointer forcing): state {e_state:.3e} vel {e_vel:.3e}")
+        assert e_state <= 1e-5 and e_vel <= 1e-5
+        assert abs(float(out[key][1][0]) / float(out["fp32"][1][0]) - 1) <= 1e-5
 
 
-def test_tc_taylor_green_decay_rate(pkg):
+@pytest.mark.parametrize("rows", ["fp32", "tc"])
+def test_tc_taylor_green_decay_rate(pkg, rows):
     """Taylor-Green through the tensor-core step at 1024^2: the (2,2) mode decays as
     exp(-nu |k|^2 t) to 1e-5 (the Jacobian error of the split-FP16 transforms feeds
     straight into that mode)."""
@@ -592,6 +610,8 @@ def test_tc_taylor_green_decay_rate(pkg):
     xs = np.arange(n) * 2 * np.pi / n
     gx, gy = np.meshgrid(xs, xs, indexing="xy")
     s = pkg.Solver.create(n=n, dyeScale=1, fft="tc-f16")
+    if rows == "tc":
+        _tc_rows(s)
     try:
         s.configure(config(viscosity=rate_for(nu, n, 1), hyperP=1))
         s.seedPhysical(6.0 * np.cos(2 * gx) * np.cos(2 * gy))
@@ -603,7 +623,7 @@ def test_tc_taylor_green_decay_rate(pkg):
         nu_h = s.paramsF[2]
         expected = np.exp(-float(nu_h) * 8.0 * dt * steps)
         err = abs(abs(w1 / w0) / expected - 1)
-        print(f"tc Taylor-Green decay-rate error {err:.3e}")
+        print(f"tc rows={rows} Taylor-Green decay-rate error {err:.3e}")
         assert err <= 1e-5
     finally:
         s.destroy()
