@@ -466,114 +466,5 @@ __global__ void __launch_bounds__(kTcThreads) k_fft_tc(float2* data, const char*
   tc_teardown(tmem);
 }
 
-// ---------------------------------------------------------------------------------------
-// Fused physical-column stage at 1024^2 with both y-transforms on the tensor cores
-// (the tcgen05 counterpart of k_phys_cols): a CTA owns 4 columns x0..x0+3.
-//   lines 0-3 = PA columns, 4-7 = PB columns -> one 8-line inverse transform; the PA
-//   and PB lines of a column then sit 4 lanes apart in one warp (shuffle exchange)
-//   (u omega, v omega) of the 4 columns -> one 4-line forward transform -> in-band Z rows
-// MODE 0 = prime (velocity + speed only), 1 = stage, 2 = last stage (+ velocity, speed).
-// Shared memory after the inverse transform: the (u, v) staging tile over the block-1
-// operand planes (y < 512 in the hi plane, y >= 512 in the lo plane), the forward
-// operands in block 0, the Z staging tile over block 0 once the GEMMs are done.
-constexpr int kTcCols = 4;
-constexpr int kTcColsGrid = 1024 / kTcCols;
-constexpr int kTcColsSmem = kTcSmem;
-
-// (y, col) -> float2 slot of a [1024][4] staging tile; the XOR spreads a warp's writes
-// (4 columns x 8 consecutive y) over all banks
-__device__ __forceinline__ int cols_stage_idx(int y, int col) { return 4 * y + (col ^ ((y >> 2) & 3)); }
-__device__ __forceinline__ float2* vel_stage_slot(char* sm, int y, int col) {
-  char* base = sm + (y < 512 ? kTcAHi + kBlockBytes : kTcALo + kBlockBytes);
-  return reinterpret_cast<float2*>(base) + cols_stage_idx(y & 511, col);
-}
-
-template <int MODE, class P = PrecF16>
-__global__ void __launch_bounds__(kTcThreads, 2) k_phys_cols_tc(PhysArgs a, const char* __restrict__ tab, int* err) {
-  constexpr int N = 1024;
-  extern __shared__ __align__(1024) char sm[];
-  const TcMisc m = tc_misc(sm);
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int x0 = blockIdx.x * kTcCols;
-  phys_latch(a);
-  // load: thread (line g, n1 t) takes the pack at ky = t + 32 n2 -- one operand row
-  const int g = tid & 7, t = tid >> 3;
-  const float2* src = (g < kTcCols ? a.pa : a.pb) + x0 + (g & (kTcCols - 1));
-  float2 v[32];
-  float mx = 0.f;
-  int nz[32];
-#pragma unroll
-  for (int n2 = 0; n2 < 32; ++n2) nz[n2] = a.row_nz ? __ldg(a.row_nz + t + 32 * n2) : 1;
-#pragma unroll
-  for (int n2 = 0; n2 < 32; ++n2) {
-    v[n2] = nz[n2] ? __ldcs(src + (size_t)(t + 32 * n2) * N) : make_float2(0.f, 0.f);   // flagged rows are zero
-    mx = fmaxf(mx, fmaxf(fabsf(v[n2].x), fabsf(v[n2].y)));
-  }
-  tc_setup<true, MODE != 0>(sm, m, tab);
-  warp_max_slot(mx, m.red);
-  __syncthreads();
-  const float scale = pow2_scale(cta_max_slots(m.red));
-  const uint32_t tmem = *m.tslot;
-#pragma unroll
-  for (int kc = 0; kc < 8; ++kc)
-    put_c4<P>(sm + kTcAHi, sm + kTcALo, t * 8 + g, kc, v[4 * kc], v[4 * kc + 1], v[4 * kc + 2], v[4 * kc + 3], scale);
-  tc_wait_tables(m, err);
-  float2 x[32];
-  fft1024_gemms<+1, 8, P>(sm, tmem, m.bar, 0u, scale, err, x);
-  // thread: line = lane & 7 (PA column c = line & 3 for line < 4, PB column for line >= 4),
-  // k2 = TcGeom<8>::index(); x[k1] at y = k2 + 32 k1.  The partner line is lane ^ 4.
-  const bool is_pa = (lane & 4) == 0;
-  const int c = lane & 3, k2 = TcGeom<8>::index();
-  float speed = 0.f, mz = 0.f;
-#pragma unroll
-  for (int k1 = 0; k1 < 32; ++k1) {
-    const float px = __shfl_xor_sync(0xffffffffu, x[k1].x, 4);
-    const float py = __shfl_xor_sync(0xffffffffu, x[k1].y, 4);
-    const float om = is_pa ? x[k1].x : px, u = is_pa ? x[k1].y : py, w = is_pa ? px : x[k1].x;
-    if (MODE != 1 && is_pa) {
-      *vel_stage_slot(sm, k2 + 32 * k1, c) = make_float2(u, w);
-      speed = fmaxf(speed, fabsf(u) + fabsf(w));
-    }
-    x[k1] = make_float2(u * om, w * om);
-    mz = fmaxf(mz, fmaxf(fabsf(x[k1].x), fabsf(x[k1].y)));
-  }
-  if (MODE != 0) warp_max_slot(mz, m.red);
-  __syncthreads();   // staged velocity and the product maxima are visible
-  if (MODE != 1) {
-#pragma unroll 4
-    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
-      const int y = i >> 2, cc = i & 3;
-      a.vel[(size_t)y * N + x0 + cc] = *vel_stage_slot(sm, y, cc);
-    }
-  }
-  if (MODE != 0) {
-    const float scale_z = pow2_scale(cta_max_slots(m.red));
-    // forward operand: row (n1 = k2, c), K = n2 = k1; the PA lane writes k1 0-15, its
-    // PB partner (same products) k1 16-31
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float2 z0 = is_pa ? x[4 * q] : x[16 + 4 * q], z1 = is_pa ? x[4 * q + 1] : x[16 + 4 * q + 1];
-      const float2 z2 = is_pa ? x[4 * q + 2] : x[16 + 4 * q + 2], z3 = is_pa ? x[4 * q + 3] : x[16 + 4 * q + 3];
-      put_c4<P>(sm + kTcAHi, sm + kTcALo, k2 * 4 + c, is_pa ? q : 4 + q, z0, z1, z2, z3, scale_z);
-    }
-    float2 zf[16];
-    fft1024_gemms<-1, 4, P>(sm, tmem, m.bar, 0u, scale_z, err, zf);
-    // thread: column c' = lane & 3, k2' = TcGeom<4>::index(); Z(ky = k2' + 32 (col0 + j))
-    using G4 = TcGeom<4>;
-    const int cz = G4::line(), kz = G4::index(), c0 = G4::col0();
-    float2* sz = reinterpret_cast<float2*>(sm);   // over the dead operands
-#pragma unroll
-    for (int j = 0; j < 16; ++j) sz[cols_stage_idx(kz + 32 * (c0 + j), cz)] = zf[j];
-    __syncthreads();
-#pragma unroll 4
-    for (int i = tid; i < N * kTcCols; i += kTcThreads) {
-      const int row = i >> 2, cc = i & 3;
-      if (fabsf(wn<N>(row)) < Tune<N>::KCUT) a.z[(size_t)row * N + x0 + cc] = sz[cols_stage_idx(row, cc)];
-    }
-  }
-  tc_teardown(tmem);
-  if (MODE != 1) cols_speed_finalize<kTcThreads>(a, speed);
-}
-
 }  // namespace tc
 }  // namespace s2d
