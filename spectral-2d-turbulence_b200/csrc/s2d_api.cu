@@ -19,6 +19,7 @@
 #include "s2d_ops.cuh"
 #include "s2d_tc.cuh"
 #include "s2d_tc_cols.cuh"
+#include "s2d_tc_lines.h"
 #include "s2d_render.cuh"
 
 using namespace s2d;
@@ -195,9 +196,11 @@ struct s2d_solver {
 
 // Row-stage variants of a solver: the registered FP32 shapes, plus (last index) the row
 // stage on the tensor cores for a tensor-core solver.
-static int spec_variants(const s2d_solver* s) { return s->ops->n_spec + (s->fft_precision != S2D_FFT_FP32 ? 1 : 0); }
+static int spec_variants(const s2d_solver* s) {
+  return s->ops->n_spec + (s->fft_precision != S2D_FFT_FP32 && s->n == 1024 ? 1 : 0);
+}
 static bool tc_rows(const s2d_solver* s) {
-  return s->fft_precision != S2D_FFT_FP32 && s->spec_choice == s->ops->n_spec;
+  return s->fft_precision != S2D_FFT_FP32 && s->n == 1024 && s->spec_choice == s->ops->n_spec;
 }
 
 // Stage-kernel shapes chosen by s2d_autotune, per (device, n, FFT precision), shared by
@@ -460,8 +463,8 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   if (dye_scale < 1 || dye_scale > 4) return fail(S2D_ERR_ARG, "dye_scale must be 1..4");
   if (fft_precision != S2D_FFT_FP32 && fft_precision != S2D_FFT_TC_F16 && fft_precision != S2D_FFT_TC_BF16)
     return fail(S2D_ERR_ARG, "unknown FFT arithmetic (S2D_FFT_FP32, S2D_FFT_TC_F16, S2D_FFT_TC_BF16)");
-  if (fft_precision != S2D_FFT_FP32 && n != 1024)
-    return fail(S2D_ERR_UNSUPPORTED_N, "the tensor-core FFT is built for N = 1024");
+  if (fft_precision != S2D_FFT_FP32 && n != 1024 && !tc::tc_lines_supported(n))
+    return fail(S2D_ERR_UNSUPPORTED_N, "the tensor-core FFT is built for N = 256, 512, 1024, 2048, 4096");
   if (int rc = check_device(device)) return rc;
   DeviceGuard guard(device);
   s2d_solver* s = new s2d_solver();
@@ -523,8 +526,10 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
                              (int)DyeGeom<64>::smem(n, s->m)), "dye kernel attributes");
   TRY(cudaFuncSetAttribute(k_dye_fused<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)DyeGeom<32>::smem(n, s->m)), "dye kernel attributes");
-  if (fft_precision == S2D_FFT_TC_F16) TRY(tc_attrs<tc::PrecF16>(), "tensor-core kernel attributes");
-  if (fft_precision == S2D_FFT_TC_BF16) TRY(tc_attrs<tc::PrecBF16>(), "tensor-core kernel attributes");
+  if (fft_precision == S2D_FFT_TC_F16 && n == 1024) TRY(tc_attrs<tc::PrecF16>(), "tensor-core kernel attributes");
+  if (fft_precision == S2D_FFT_TC_BF16 && n == 1024) TRY(tc_attrs<tc::PrecBF16>(), "tensor-core kernel attributes");
+  if (fft_precision != S2D_FFT_FP32 && n != 1024)
+    TRY(tc::tc_lines_attrs(n, fft_precision == S2D_FFT_TC_BF16), "tensor-core kernel attributes");
   // zero everything the reference's fresh buffers hold as zero
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->state[i], 0, cbytes, s->stream), "memset");
   TRY(cudaMemsetAsync(s->packA, 0, cbytes, s->stream), "memset");
@@ -539,10 +544,14 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   for (int i = 0; i < 3; ++i) TRY(cudaMemsetAsync(s->dye[i], 0, dbytes, s->stream), "memset");
   k_twiddles<<<(n + 255) / 256, 256, 0, s->stream>>>(s->tw, n);
   TRY(cudaGetLastError(), "twiddle kernel");
-  if (fft_precision != S2D_FFT_FP32) {
+  if (fft_precision != S2D_FFT_FP32 && n == 1024) {
     TRY(cudaMalloc(&s->tctab, tc::kTabBytes), "tensor-core tables");
     if (fft_precision == S2D_FFT_TC_BF16) tc::k_tc_tables<tc::PrecBF16><<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
     else tc::k_tc_tables<tc::PrecF16><<<1, 256, 0, s->stream>>>(s->tctab, s->tw);
+    TRY(cudaGetLastError(), "tensor-core table kernel");
+  } else if (fft_precision != S2D_FFT_FP32) {
+    TRY(cudaMalloc(&s->tctab, tc::tc_lines_table_bytes(n)), "tensor-core tables");
+    tc::tc_lines_tables(n, fft_precision == S2D_FFT_TC_BF16, s->tctab, s->tw, s->stream);
     TRY(cudaGetLastError(), "tensor-core table kernel");
   }
   // an unconfigured solver has all-zero parameters apart from the grid constants
@@ -704,8 +713,10 @@ static inline unsigned cells_grid(int n) { return (unsigned)(((size_t)n * n + 25
 
 static int enqueue_fft2(s2d_solver* s, float2* buf, int sign) {
   if (is_tc(s)) {
-    // tensor-core DFT-GEMM passes, 8 lines of 1024 per CTA
-    if (s->fft_precision == S2D_FFT_TC_BF16) tc_fft2_launch<tc::PrecBF16>(buf, sign, s->tctab, s->err, s->stream);
+    // tensor-core DFT-GEMM passes: 8 lines of 1024 per CTA, or the generic N1 x N2 form
+    if (s->n != 1024)
+      tc::tc_lines_fft2(s->n, s->fft_precision == S2D_FFT_TC_BF16, buf, sign, s->tctab, s->tw, s->err, s->stream);
+    else if (s->fft_precision == S2D_FFT_TC_BF16) tc_fft2_launch<tc::PrecBF16>(buf, sign, s->tctab, s->err, s->stream);
     else tc_fft2_launch<tc::PrecF16>(buf, sign, s->tctab, s->err, s->stream);
     S2D_LAUNCHED();
     return S2D_OK;
@@ -776,9 +787,65 @@ static void enqueue_phys_cols(s2d_solver* s, int mode, const PhysArgs& a) {
 
 extern "C" int s2d_encode_reduce(s2d_solver* s);
 
+// Tensor-core solvers at the sizes without fused tensor-core stage kernels (N != 1024) run
+// the reference's per-stage order (solver.js:488-521): velocity pack, two inverse 2D
+// transforms, products, forward transform, assemble, RK3 update -- with every 2D transform
+// on the tensor cores (s2d_tc_lines.cu) and the pointwise stages on the CUDA cores.
+static bool tc_unfused(const s2d_solver* s) { return is_tc(s) && s->n != 1024; }
+
+// velocity (and the packs' physical fields) of state `idx` through the unfused stages
+static int enqueue_unfused_velocity(s2d_solver* s, int idx) {
+  const unsigned g = cells_grid(s->n);
+  k_velocity_pack<<<g, 256, 0, s->stream>>>(s->state[idx], s->packA, s->packB, s->n);
+  S2D_LAUNCHED();
+  if (int rc = enqueue_fft2(s, s->packA, +1)) return rc;
+  if (int rc = enqueue_fft2(s, s->packB, +1)) return rc;
+  k_nl_pack<<<g, 256, 0, s->stream>>>(s->packA, s->packB, s->physZ, s->vel, s->n);
+  S2D_LAUNCHED();
+  return S2D_OK;
+}
+
+static int enqueue_unfused_step(s2d_solver* s, bool ptr) {
+  if (s->latch_pending) {
+    k_latch_step<<<1, 1, 0, s->stream>>>(s->dparams, s->step_counter);
+    S2D_LAUNCHED();
+    s->latch_pending = false;
+  }
+  const int p = s->phase;
+  const unsigned g = cells_grid(s->n);
+  const float* dt = dt_slot(s, s->slot);
+  for (int st = 0; st < 3; ++st) {
+    if (int rc = enqueue_unfused_velocity(s, (p + st) % 3)) return rc;
+    if (int rc = enqueue_fft2(s, s->physZ, -1)) return rc;
+    k_assemble<<<g, 256, 0, s->stream>>>(s->physZ, ptr ? s->force : nullptr, dt, s->dparams, s->rhs, s->n);
+    S2D_LAUNCHED();
+    float2* w0 = s->state[p];
+    float2* wc = s->state[(p + st) % 3];
+    float2* wo = s->state[(p + (st == 1 ? 2 : 1)) % 3];
+    if (st == 0) k_rk3<0><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+    else if (st == 1) k_rk3<1><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+    else k_rk3<2><<<g, 256, 0, s->stream>>>(w0, wc, wo, s->rhs, dt, s->dparams, s->n);
+    S2D_LAUNCHED();
+  }
+  s->reduced_valid = false;   // the CFL reduction runs as its own two launches
+  s->packs_valid = false;
+  s->packs_flagged = false;
+  s->phase = (p + 1) % 3;
+  s->step_index += 1;
+  return S2D_OK;
+}
+
 extern "C" int s2d_encode_prime(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
+  if (tc_unfused(s)) {
+    if (int rc = materialize_packs(s)) return rc;
+    if (int rc = enqueue_unfused_velocity(s, s->phase)) return rc;
+    s->reduced_valid = false;
+    if (int rc = s2d_encode_reduce(s)) return rc;
+    s->primed = true;
+    return S2D_OK;
+  }
   if (int rc = enqueue_pack_prime(s)) return rc;
   PhysArgs a = phys_args(s, 1);
   enqueue_phys_cols(s, 0, a);
@@ -792,7 +859,7 @@ extern "C" int s2d_encode_prime(s2d_solver* s) {
 extern "C" int s2d_encode_step(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
-  if (!s->packs_valid)
+  if (!s->packs_valid && !tc_unfused(s))
     if (int rc = enqueue_pack_prime(s)) return rc;
   const bool ptr = s->hs.count > 0;
   if (ptr) {
@@ -800,6 +867,10 @@ extern "C" int s2d_encode_step(s2d_solver* s) {
     k_pointer_force<<<cells_grid(s->n), 256, 0, s->stream>>>(s->force, s->dsplats, s->n);
     S2D_LAUNCHED();
     if (int rc = enqueue_fft2(s, s->force, -1)) return rc;
+  }
+  if (tc_unfused(s)) {
+    if (int rc = materialize_packs(s)) return rc;
+    return enqueue_unfused_step(s, ptr);
   }
   const int p = s->phase;
   for (int st = 0; st < 3; ++st) {
@@ -936,7 +1007,7 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
   DeviceGuard guard(s->dev);
   if (!s->primed)
     if (int rc = s2d_encode_prime(s)) return rc;
-  if (!s->packs_valid)
+  if (!s->packs_valid && !tc_unfused(s))
     if (int rc = enqueue_pack_prime(s)) return rc;
   if (flags & S2D_STEP_RELATCH)
     if (int rc = sync_step_counter(s)) return rc;

@@ -553,10 +553,18 @@ static __global__ void k_assemble(const float2* __restrict__ physz, const float2
   const float2 q2 = make_float2(0.5f * dd.y, -0.5f * dd.x);
   const float2 nhat = make_float2(-(kx * q1.y) - ky * q2.y, kx * q1.x + ky * q2.x);
   const float mask = (fabsf(kx) < P.kcut && fabsf(ky) < P.kcut) ? 1.f : 0.f;
-  float2 f = cscale(csub(fhat[idx], nhat), mask);
+  float2 f = cscale(csub(fhat ? fhat[idx] : make_float2(0.f, 0.f), nhat), mask);   // no pointer force: nullptr
   if (P.force_amp > 0.f && mask > 0.f && k2 > 0.f)
     f = cadd(f, stochastic_term(P, n, row, col, kx, ky, k2, dtbuf[0]));
   rhs[idx] = f;
+}
+
+// the per-substep stepIndex latch (S2D_STEP_RELATCH) as a launch of its own, for steps
+// whose first kernel is not the fused column kernel that otherwise performs it
+static __global__ void k_latch_step(DevParams* params, uint32_t* counter) {
+  const uint32_t k = *counter;
+  params->step_index = k;
+  *counter = k + 1u;
 }
 
 template <int S>

@@ -456,11 +456,65 @@ def test_tc_fft2_matches_numpy(pkg):
         s.destroy()
 
 
-def test_tc_precision_only_at_1024(pkg):
+def test_tc_precision_sizes(pkg):
+    """The tensor-core FFT exists at 256, 512, 1024, 2048 and 4096; smaller grids are
+    refused with S2D_ERR_UNSUPPORTED_N."""
     for fft in ("tc-f16", "tc-bf16"):
-        with pytest.raises(pkg.S2DError) as ei:
-            pkg.Solver.create(n=512, fft=fft)
-        assert ei.value.status == -2
+        for n in (32, 64, 128):
+            with pytest.raises(pkg.S2DError) as ei:
+                pkg.Solver.create(n=n, fft=fft)
+            assert ei.value.status == -2
+
+
+@pytest.mark.parametrize("n", [256, 512, 2048, 4096])
+@pytest.mark.parametrize("fft", ["tc-f16", "tc-bf16"])
+def test_tc_generic_fft2_matches_numpy(pkg, n, fft):
+    """The N1 x N2 tensor-core 2D transforms (the grid sizes other than 1024), forward
+    unscaled and inverse scaled 1/N per pass (fft.js:58-59), against numpy in FP64."""
+    rng = np.random.default_rng(n)
+    a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+    try:
+        s.setBuffer("packB", a)
+        s.fft.forward(None, "packB")
+        e_fwd = rel_l2(s.getBuffer("packB"), np.fft.fft2(a.astype(np.complex128)))
+        s.setBuffer("packB", a)
+        s.fft.inverse(None, "packB")
+        e_inv = rel_l2(s.getBuffer("packB"), np.fft.ifft2(a.astype(np.complex128)))
+        s.synchronize()
+    finally:
+        s.destroy()
+    print(f"{fft} {n}^2 2D FFT rel L2: forward {e_fwd:.3e} inverse {e_inv:.3e}")
+    bound = 5e-6 if fft == "tc-f16" else 2e-5
+    assert e_fwd <= bound and e_inv <= bound
+
+
+@pytest.mark.parametrize("n", [256, 512, 2048])
+@pytest.mark.parametrize("fft", ["tc-f16", "tc-bf16"])
+def test_tc_unfused_step_vs_oracle(pkg, n, fft):
+    """Tensor-core solvers at the sizes without fused tensor-core stages run the reference's
+    per-stage order with every 2D transform on the tensor cores: rel L2 to the FP64 oracle
+    <= 1e-5 after one step (beta, hyperviscosity, drag), <= 3e-5 after three."""
+    mu, p, dt, beta = 1e-2, 4, 1e-3, 10.0
+    nu_h = 1.0 / (n / 3.0) ** 8
+    ref = SpectralOracle(n=n, beta=beta, mu=mu, nu_h=nu_h, hyper_p=p)
+    ref.set_vorticity(random_field(n, k0=n / 16, seed=13, amplitude=8.0))
+    w_in = ref.w.astype(np.complex64)
+    ref.w = w_in.astype(np.complex128)
+    s = _tc_case_solver(pkg, fft, n, beta, mu, nu_h, p, w_in, dt)
+    try:
+        s.encodeStep()
+        ref.step(dt=dt)
+        err1 = rel_l2(current_state(s), ref.w)
+        for _ in range(2):
+            s.encodeStep()
+            ref.step(dt=dt)
+        err3 = rel_l2(current_state(s), ref.w)
+        s.synchronize()
+    finally:
+        s.destroy()
+    print(f"{fft} {n}^2 unfused tensor-core step rel L2: 1 step {err1:.3e}, 3 steps {err3:.3e}")
+    assert err1 <= 1e-5 and err3 <= 3e-5
 
 
 def test_precision_sweep_fft_and_step(pkg):
