@@ -84,7 +84,7 @@ __device__ __forceinline__ float2 lerp2v(float2 a, float2 b, float t) {
 // bilinear velocity at normalised p (dye.wgsl:27-38); cell indices wrapped
 template <class VF>
 __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, int n) {
-  const float nf = (float)n;
+  const float nf = int_to_f(n);
   const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
   int ix, iy;
   const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
@@ -127,7 +127,7 @@ struct Footprint {
   float fx, fy;
 };
 __device__ __forceinline__ Footprint footprint(float sx, float sy, int m) {
-  const float mf = (float)m;
+  const float mf = int_to_f(m);
   const float gx = __fmaf_rn(sx, mf, -0.5f), gy = __fmaf_rn(sy, mf, -0.5f);   // sx * mf exact
   int ix, iy;
   const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
@@ -166,7 +166,7 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
 // texel centre (x + 0.5)/m; m is a power of two, so x/m, 0.5/m and their sum (2x+1)/(2m)
 // are all exact and one fused multiply-add gives the quotient
 __device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
-  const float inv = __frcp_rn((float)m);
+  const float inv = __int_as_float((128 - __ffs(m)) << 23);   // 2^-log2(m): exactly 1/m, no XU reciprocal
   const float half_inv = 0.5f * inv;
   return make_float2(__fmaf_rn(int_to_f(x), inv, half_inv), __fmaf_rn(int_to_f(y), inv, half_inv));
 }
@@ -324,7 +324,7 @@ struct SmemVel {
 // bilinear velocity with one window test for the 2x2 cell footprint (same arithmetic as sample_vel)
 __device__ __forceinline__ float2 sample_vel_win(const SmemVel& vf, float px, float py) {
   const int n = vf.n;
-  const float nf = (float)n;
+  const float nf = int_to_f(n);
   const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
   int ix, iy;
   const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
