@@ -63,9 +63,12 @@ enum s2d_buffer_id {
 
 /* FFT arithmetic of the fused step */
 #define S2D_FFT_FP32 0            /* CUDA-core FP32 FFT */
-#define S2D_FFT_TC_F16 1          /* tensor-core DFT-GEMM, FP16 hi+lo split, FP32 accumulate (N = 1024) */
-#define S2D_FFT_TC_BF16 2         /* tensor-core DFT-GEMM, BF16 hi+lo split, FP32 accumulate (N = 1024):
-                                     16 significant bits per operand (the FP16 split keeps 22) */
+/* Tensor-core DFT-GEMM FFT with split hi+lo operands and FP32 accumulation, N = 256, 512,
+ * 1024, 2048, 4096 (other N: S2D_ERR_UNSUPPORTED_N).  At N = 1024 the step's stages are
+ * fused tensor-core kernels; at the other sizes the step runs the reference's per-stage
+ * order with every 2D transform on the tensor cores. */
+#define S2D_FFT_TC_F16 1          /* FP16 hi+lo: 22 significant bits per operand */
+#define S2D_FFT_TC_BF16 2         /* BF16 hi+lo: 16 significant bits per operand */
 
 /* dye patterns of paintDye (solver.js:446-473) */
 #define S2D_DYE_NONE 0

@@ -105,7 +105,10 @@ class Solver:
     # ---------------------------------------------------------------- lifecycle
     @staticmethod
     def create(device: int = 0, n: int = 256, dyeScale: int = 2, fft: str = "fp32") -> "Solver":
-        """solver.js:71-75 (``create(device, {n, dyeScale})``); ``fft`` selects the FFT arithmetic."""
+        """solver.js:71-75 (``create(device, {n, dyeScale})``); ``fft`` selects the FFT arithmetic:
+        "fp32" (CUDA cores, every size) or the tensor-core split forms "tc-f16" / "tc-bf16"
+        (N = 256, 512, 1024, 2048, 4096; fused stage kernels at 1024^2, the reference's
+        per-stage order with tensor-core 2D transforms at the other sizes)."""
         if fft not in _PRECISIONS:
             raise ValueError(f"unknown FFT arithmetic {fft!r}")
         h = C.c_void_p()
