@@ -185,11 +185,13 @@ __device__ __forceinline__ float cta_max(float v, unsigned* word) {
   return __uint_as_float(*word);
 }
 
-// power-of-two scale that maps max |x| into [2^13, 2^14) (FP16 max is 65504)
+// power-of-two scale that maps max |x| into [2^13, 2^14) (FP16 max is 65504), at most 2^126:
+// a row of subnormal values (the far field of a localised vortex) would otherwise ask for
+// a scale beyond FP32 range (inf, and inf * 0 = NaN); 2^126 and its inverse stay normal
 __device__ __forceinline__ float pow2_scale(float maxabs) {
   if (!(maxabs > 0.f) || !isfinite(maxabs)) return 1.f;
   const int e = ilogbf(maxabs);                       // maxabs in [2^e, 2^(e+1))
-  return ldexpf(1.f, 13 - e);
+  return ldexpf(1.f, min(13 - e, 126));
 }
 
 }  // namespace tc
