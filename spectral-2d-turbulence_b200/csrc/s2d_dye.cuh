@@ -60,20 +60,6 @@ struct GlobalVel {
 __device__ __forceinline__ float lerp1(float a, float b, float t) {
   return __fmaf_rn(b, t, __fmul_rn(a, __fsub_rn(1.f, t)));   // WGSL mix(a, b, t)
 }
-// floor(x) and its integer for |x| < 2^22 on the FMA / ALU pipes instead of the XU pipe:
-// x + 1.5 * 2^23 rounded toward -infinity is floor(x) + 1.5 * 2^23 exactly (the sum lies in
-// [2^23, 2^24), whose spacing is 1), and that float's bits are 0x4B400000 + floor(x).  The
-// value equals floorf(x) bit for bit except for x = -0 (floorf keeps the sign): the
-// coordinates passed here are round-to-nearest sums and products, which are never -0.
-__device__ __forceinline__ float floor_fi(float x, int* i) {
-  const float t = __fadd_rd(x, 12582912.f);
-  *i = __float_as_int(t) - 0x4B400000;
-  return __fsub_rn(t, 12582912.f);
-}
-__device__ __forceinline__ float floor_f(float x) { return __fsub_rn(__fadd_rd(x, 12582912.f), 12582912.f); }
-// (float)i for |i| < 2^22, exact, without the XU conversion
-__device__ __forceinline__ float int_to_f(int i) { return __fsub_rn(__int_as_float(0x4B400000 + i), 12582912.f); }
-
 // lerp1 on two channels at once with the packed FP32x2 pipe (sm_100): each lane is the
 // same correctly rounded multiply and fused multiply-add, so the bits equal lerp1's
 __device__ __forceinline__ float2 lerp2v(float2 a, float2 b, float t) {
@@ -84,11 +70,11 @@ __device__ __forceinline__ float2 lerp2v(float2 a, float2 b, float t) {
 // bilinear velocity at normalised p (dye.wgsl:27-38); cell indices wrapped
 template <class VF>
 __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, int n) {
-  const float nf = int_to_f(n);
+  const float nf = (float)n;
   const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
-  int ix, iy;
-  const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
+  const float bx = floorf(gx), by = floorf(gy);
   const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
+  const int ix = (int)bx, iy = (int)by;
   const int x0 = ix & (n - 1), x1 = (ix + 1) & (n - 1), y0 = iy & (n - 1), y1 = (iy + 1) & (n - 1);
   const float2 v00 = vf(x0, y0), v10 = vf(x1, y0), v01 = vf(x0, y1), v11 = vf(x1, y1);
   return lerp2v(lerp2v(v00, v10, fx), lerp2v(v01, v11, fx), fy);
@@ -96,7 +82,7 @@ __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, i
 
 __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - d + 1)
   const float x = __fadd_rn(__fsub_rn(p, d), 1.f);
-  return __fsub_rn(x, floor_f(x));
+  return __fsub_rn(x, floorf(x));
 }
 
 // midpoint back-trace (dye.wgsl:40-45), from the velocity v1 already sampled at p
@@ -106,7 +92,7 @@ __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - 
 __device__ __forceinline__ float2 fract_shift2(float2 p, float2 v, float s) {
   const float2 d = __fmul2_rn(v, make_float2(-s, -s));
   const float2 x = __fadd2_rn(__fadd2_rn(p, d), make_float2(1.f, 1.f));
-  return make_float2(__fsub_rn(x.x, floor_f(x.x)), __fsub_rn(x.y, floor_f(x.y)));
+  return make_float2(__fsub_rn(x.x, floorf(x.x)), __fsub_rn(x.y, floorf(x.y)));
 }
 template <class VF>
 __device__ __forceinline__ float2 trace_from(const VF& vf, float px, float py, float2 v1, float h, int n) {
@@ -127,17 +113,16 @@ struct Footprint {
   float fx, fy;
 };
 __device__ __forceinline__ Footprint footprint(float sx, float sy, int m) {
-  const float mf = int_to_f(m);
+  const float mf = (float)m;
   const float gx = __fmaf_rn(sx, mf, -0.5f), gy = __fmaf_rn(sy, mf, -0.5f);   // sx * mf exact
-  int ix, iy;
-  const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
+  const float bx = floorf(gx), by = floorf(gy);
   Footprint f;
   f.fx = __fsub_rn(gx, bx);
   f.fy = __fsub_rn(gy, by);
-  f.x0 = ix & (m - 1);
-  f.x1 = (ix + 1) & (m - 1);
-  f.y0 = iy & (m - 1);
-  f.y1 = (iy + 1) & (m - 1);
+  f.x0 = (int)bx & (m - 1);
+  f.x1 = ((int)bx + 1) & (m - 1);
+  f.y0 = (int)by & (m - 1);
+  f.y1 = ((int)by + 1) & (m - 1);
   return f;
 }
 
@@ -166,9 +151,9 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
 // texel centre (x + 0.5)/m; m is a power of two, so x/m, 0.5/m and their sum (2x+1)/(2m)
 // are all exact and one fused multiply-add gives the quotient
 __device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
-  const float inv = __int_as_float((128 - __ffs(m)) << 23);   // 2^-log2(m): exactly 1/m, no XU reciprocal
+  const float inv = __frcp_rn((float)m);
   const float half_inv = 0.5f * inv;
-  return make_float2(__fmaf_rn(int_to_f(x), inv, half_inv), __fmaf_rn(int_to_f(y), inv, half_inv));
+  return make_float2(__fmaf_rn((float)x, inv, half_inv), __fmaf_rn((float)y, inv, half_inv));
 }
 
 // BFECC correction of one texel from its source (a, with the 4-texel min/max) and
@@ -324,11 +309,11 @@ struct SmemVel {
 // bilinear velocity with one window test for the 2x2 cell footprint (same arithmetic as sample_vel)
 __device__ __forceinline__ float2 sample_vel_win(const SmemVel& vf, float px, float py) {
   const int n = vf.n;
-  const float nf = int_to_f(n);
+  const float nf = (float)n;
   const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
-  int ix, iy;
-  const float bx = floor_fi(gx, &ix), by = floor_fi(gy, &iy);
+  const float bx = floorf(gx), by = floorf(gy);
   const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
+  const int ix = (int)bx, iy = (int)by;
   const int rx = (ix - vf.ox) & (n - 1), ry = (iy - vf.oy) & (n - 1);
   float2 v00, v10, v01, v11;
   if (rx + 1 < vf.w && ry + 1 < vf.wy) {
