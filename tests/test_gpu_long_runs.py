@@ -144,6 +144,46 @@ def test_config1_taylor_green_256(pkg, fft):
     _taylor_green(pkg, 256, 1000, fft, jac_bound=b, rate_bound=b)
 
 
+# ---------------------------------------------------------------- configuration 2
+@pytest.mark.parametrize("n", [1024, 2048])
+def test_config2_forced_inverse_cascade(pkg, n):
+    """Forced inverse cascade at 1024^2 and 2048^2, every FFT path against one FP64 run:
+    white-in-time forcing |k| = 64 +- 2 at amplitude 0.1, order-4 hyperviscosity at damping
+    rate 1 at the cutoff (the written nu4 = 1e-16 overflows E(-dt/2) in FP32 at 1024^2),
+    drag 1e-2, beta 0, the benchmark's band seed (4 <= |k| <= 12, rms 1), dt = 5e-4 fixed
+    (inside the CFL 0.5 limit of this flow; a fixed dt keeps the forcing amplitude, which
+    scales as dt^-1/2, identical between the runs), 2000 steps."""
+    dt, steps = 5e-4, 2000
+    cfg = config(drag=1e-2, viscosity=1.0, hyperP=4, forceAmp=0.1, forceK=64.0, forceWidth=2.0)
+    got, w0, nu_h = {}, None, None
+    for fft in FFTS:
+        s = pkg.Solver.create(n=n, dyeScale=1, fft=fft)
+        try:
+            s.configure(cfg)
+            s.seedBand(4.0, 12.0, rms=1.0, seed=1)
+            w = current_state(s)
+            if w0 is None:
+                w0, nu_h = w, float(s.paramsF[2])
+            assert np.array_equal(w, w0)
+            _run_fixed(s, steps, dt)
+            got[fft] = current_state(s)
+        finally:
+            s.destroy()
+    ref = Fp64Torch(n, mu=1e-2, nu_h=nu_h, hyper_p=4)
+    ref.set_spectrum(w0)
+    forcing = AnnulusForcing(n, 0.1, 64.0, 2.0)
+    for k in range(steps):
+        ref.step(dt, forcing(k, dt))
+    want = ref.spectrum_np()
+    del ref
+    bounds = {"fp32": 2e-5, "tc-f16": 5e-5, "tc-bf16": 2e-4}
+    for fft in FFTS:
+        err = _errors(got[fft], want)
+        _report(f"config2 n={n}", fft, err)
+        for key in ("state", "energy", "enstrophy", "spectrum"):
+            assert err[key] <= bounds[fft], f"{fft} {key} {err[key]:.3e}"
+
+
 # ---------------------------------------------------------------- configuration 4
 @pytest.mark.parametrize("fft", FFTS)
 def test_config4_beta_plane_4096(pkg, fft):
