@@ -257,8 +257,23 @@ def paint_dye_bands(m):
 
 
 # ----------------------------------------------------------------------------- dye advection
+def _fma32(a, b, c):
+    """a * b + c with one FP32 rounding, as the CUDA kernels' fused multiply-add: the
+    product of two FP32 values is exact in FP64, the sum is rounded once to FP64 and then
+    to FP32 (the two roundings can differ from one only when the FP64 sum lands exactly on
+    an FP32 rounding midpoint, which these magnitudes make vanishingly rare)."""
+    return (np.asarray(a, np.float64) * np.asarray(b, np.float64) + np.asarray(c, np.float64)).astype(F32)
+
+
+def _lerp(a, b, t):
+    """WGSL mix(a, b, t) as the kernels evaluate it: fma(b, t, a * (1 - t))."""
+    one = F32(1.0)
+    return _fma32(b, t, (a * (one - t)).astype(F32))
+
+
 def _bilinear(tex, px, py, size):
-    """Repeat-wrapped bilinear sample at normalised coords (software form of dye.wgsl:64,73,84-85)."""
+    """Repeat-wrapped bilinear sample at normalised coords (software form of dye.wgsl:64,73,84-85),
+    with the kernels' operation order (one fused multiply-add per interpolation)."""
     gx = (px * F32(size) - F32(0.5)).astype(F32)
     gy = (py * F32(size) - F32(0.5)).astype(F32)
     bx, by = np.floor(gx), np.floor(gy)
@@ -269,10 +284,9 @@ def _bilinear(tex, px, py, size):
     fx = fx[..., None] if tex.ndim == 3 else fx
     fy = fy[..., None] if tex.ndim == 3 else fy
     t00, t10, t01, t11 = tex[iy, ix], tex[iy, ix1], tex[iy1, ix], tex[iy1, ix1]
-    one = F32(1.0)
-    a = (t00 * (one - fx) + t10 * fx).astype(F32)
-    b = (t01 * (one - fx) + t11 * fx).astype(F32)
-    return (a * (one - fy) + b * fy).astype(F32)
+    a = _lerp(t00, t10, fx)
+    b = _lerp(t01, t11, fx)
+    return _lerp(a, b, fy)
 
 
 def _trace(px, py, vel, n, h):

@@ -130,10 +130,22 @@ def test_dye_bfecc_step(pkg, m_scale):
         s.encodeDye()
         got = wo.half_bits_to_f32(s.currentDye)
         velf = np.stack([vel.real, vel.imag], axis=-1).astype(np.float32)
-        want = wo.half_bits_to_f32(wo.dye_step(dye0, velf, dt, 0.999, [_splat_np(splat)]))
-        diff = np.abs(got - want)
-        assert diff.max() <= 4e-3, diff.max()
-        assert diff.mean() <= 1e-5, diff.mean()
+        want_bits = wo.dye_step(dye0, velf, dt, 0.999, [_splat_np(splat)])
+        want = wo.half_bits_to_f32(want_bits)
+        # the restatement evaluates the kernels' FP32 operations in the same order with the
+        # same fused multiply-adds: texels untouched by the splat agree bit for bit; inside
+        # the splat the weight uses expf, whose CUDA and NumPy results may differ in the
+        # last FP32 bit, which can move the binary16 result by one unit in the last place
+        px = (np.arange(n * m_scale) + 0.5) / (n * m_scale)
+        rx = (px[None, :] - splat["x"] + 0.5) % 1.0 - 0.5
+        ry = (px[:, None] - splat["y"] + 0.5) % 1.0 - 0.5
+        near = (rx * rx + ry * ry) < 9.0 * splat["radius"] ** 2 * 1.01
+        gb = s.currentDye.astype(np.int32)
+        wb = want_bits.astype(np.int32)
+        far = ~near
+        assert np.array_equal(gb[far], wb[far]), int(np.count_nonzero(gb[far] != wb[far]))
+        assert np.max(np.abs(gb[near] - wb[near])) <= 1
+        assert np.mean(gb[near] != wb[near]) <= 1e-2
         assert np.all(got[..., 3] == 1.0)
     finally:
         s.destroy()
