@@ -124,7 +124,8 @@ int s2d_wavenumber_table(int n, float* out /* n */);
 int s2d_dealias_mask_table(int n, uint8_t* out /* n*n */);
 
 /* ---------------------------------------------------------------- lifecycle */
-/* Solver.create(device, {n, dyeScale}) (solver.js:71-140). */
+/* Solver.create(device, {n, dyeScale}) (solver.js:71-140).  dye_scale is 1, 2 (the
+ * reference's two choices, main.js:196) or 4; any other value is S2D_ERR_ARG. */
 int s2d_create(int n, int dye_scale, int fft_precision, int device, s2d_solver** out);
 /* Solver.destroy() (solver.js:614-629); the handle is freed. */
 int s2d_destroy(s2d_solver* s);

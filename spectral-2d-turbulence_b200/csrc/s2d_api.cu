@@ -460,7 +460,10 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
     return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " must be a power of two");
   const NOps* ops = ops_for(n);
   if (!ops) return fail(S2D_ERR_UNSUPPORTED_N, "grid size " + std::to_string(n) + " outside 32..4096");
-  if (dye_scale < 1 || dye_scale > 4) return fail(S2D_ERR_ARG, "dye_scale must be 1..4");
+  // the dye grid must be a power of two (wrapped texel indices, exact texel centres): the
+  // reference offers dyeScale 1 and 2 (main.js:196); 4 is accepted as well
+  if (dye_scale != 1 && dye_scale != 2 && dye_scale != 4)
+    return fail(S2D_ERR_ARG, "dye_scale must be 1, 2 or 4");
   if (fft_precision != S2D_FFT_FP32 && fft_precision != S2D_FFT_TC_F16 && fft_precision != S2D_FFT_TC_BF16)
     return fail(S2D_ERR_ARG, "unknown FFT arithmetic (S2D_FFT_FP32, S2D_FFT_TC_F16, S2D_FFT_TC_BF16)");
   if (fft_precision != S2D_FFT_FP32 && n != 1024 && !tc::tc_lines_supported(n))

@@ -340,15 +340,7 @@ __device__ __forceinline__ float2 sample_vel(const WinVel& w, float px, float py
 
 // r, g, b of the bilinear sample over a footprint, optionally with the 4-texel min / max
 // (the same per-channel arithmetic as bilerp)
-template <class TF>
-__device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) {
-  Rgb q[4];
-  if (!tf.quad(f, q)) {
-    q[0] = tf(f.x0, f.y0);
-    q[1] = tf(f.x1, f.y0);
-    q[2] = tf(f.x0, f.y1);
-    q[3] = tf(f.x1, f.y1);
-  }
+__device__ __forceinline__ Rgb bilerp_quad(const Rgb (&q)[4], const Footprint& f, Rgb* lo, Rgb* hi) {
   const Rgb c00 = q[0], c10 = q[1], c01 = q[2], c11 = q[3];
   if (lo) {
     lo->r = fminf(fminf(c00.r, c10.r), fminf(c01.r, c11.r));
@@ -361,6 +353,43 @@ __device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb*
   const float2 rg = lerp2v(lerp2v(make_float2(c00.r, c00.g), make_float2(c10.r, c10.g), f.fx),
                            lerp2v(make_float2(c01.r, c01.g), make_float2(c11.r, c11.g), f.fx), f.fy);
   return {rg.x, rg.y, lerp2(c00.b, c10.b, c01.b, c11.b, f.fx, f.fy)};
+}
+template <class TF>
+__device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) {
+  Rgb q[4];
+  if (!tf.quad(f, q)) {
+    q[0] = tf(f.x0, f.y0);
+    q[1] = tf(f.x1, f.y0);
+    q[2] = tf(f.x0, f.y1);
+    q[3] = tf(f.x1, f.y1);
+  }
+  return bilerp_quad(q, f, lo, hi);
+}
+
+// Window lookups without a bounds test, for a tile whose every trace moves less than one
+// texel: each footprint then lies inside its window by construction of the halos, and the
+// lookup reads the same slots (and does the same arithmetic) as the tested one above.
+struct FastTex {   // binary16 window of row length W at wrapped origin (ox, oy)
+  const uint2* sm;
+  int w, ox, oy, m;
+  __device__ __forceinline__ Rgb sample(const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) const {
+    const uint2* p = sm + ((f.y0 - oy) & (m - 1)) * w + ((f.x0 - ox) & (m - 1));
+    const Rgb q[4] = {rgb_of(p[0]), rgb_of(p[1]), rgb_of(p[w]), rgb_of(p[w + 1])};
+    return bilerp_quad(q, f, lo, hi);
+  }
+};
+struct FastVel {   // FP32 velocity window
+  const float2* sm;
+  int w, ox, oy, n;
+};
+__device__ __forceinline__ float2 sample_vel(const FastVel& v, float px, float py, int) {
+  const int n = v.n;
+  const float nf = (float)n;
+  const float gx = __fmaf_rn(px, nf, -0.5f), gy = __fmaf_rn(py, nf, -0.5f);   // px * nf exact
+  const float bx = floorf(gx), by = floorf(gy);
+  const float fx = __fsub_rn(gx, bx), fy = __fsub_rn(gy, by);
+  const float2* p = v.sm + (((int)by - v.oy) & (n - 1)) * v.w + (((int)bx - v.ox) & (n - 1));
+  return lerp2v(lerp2v(p[0], p[1], fx), lerp2v(p[v.w], p[v.w + 1], fx), fy);
 }
 
 // binary16 W x WY window whose texels outside the window are re-derived by EVAL
@@ -423,6 +452,115 @@ __device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const R
   return correct_from(a4, b4, lo4, hi4, px, py, fade, S);
 }
 
+// Windows, origins and constants of one CTA of the fused dye kernel.
+template <int TX> struct DyeCta {
+  const float2* vel;
+  const uint2* src;
+  uint2* dst;
+  const DevSplats* S;
+  uint2 *s_src, *s_back, *s_fwd;
+  float2 *s_v1, *s_sp, *s_vel;
+  int n, m, tx0, ty0;
+  int sx0, sy0, fx0, fy0, bx0, by0;   // wrapped origins of the source / forward / backward windows
+  int vxw, vyw, vwx, vwy;             // velocity window: wrapped origin and extent
+  float h, fade;
+};
+
+// The forward, backward and corrected passes of one tile.  FAST: every trace of the tile
+// moves less than one texel (checked on the velocity window the traces read), so every
+// footprint lies inside its window and the lookups skip the bounds tests and the
+// recomputation from global memory; the arithmetic, and so the bits, are the same.
+template <int TX, bool FAST>
+__device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
+  using G = DyeGeom<TX>;
+  constexpr int TY = G::TY, NT = G::THREADS;
+  constexpr int W1X = G::W1X, W1Y = G::W1Y, W2X = G::W2X, W2Y = G::W2Y, W3X = G::W3X, W3Y = G::W3Y;
+  const int tid = threadIdx.x;
+  const int n = c.n, m = c.m;
+  const float h = c.h;
+  const SmemVel V{c.s_vel, c.vxw, c.vyw, c.vwx, c.vwy, n, c.vel};
+  const FastVel FV{c.s_vel, c.vwx, c.vxw, c.vyw, n};
+  auto vel_at = [&](float px, float py) {
+    if constexpr (FAST) return sample_vel(FV, px, py, n);
+    else return sample_vel_win(V, px, py);
+  };
+  auto trace = [&](float px, float py, float2 v1, float hs) {
+    if constexpr (FAST) return trace_from(FV, px, py, v1, hs, n);
+    else return trace_from(WinVel{V}, px, py, v1, hs, n);
+  };
+  using Tex = SmemTex<W3X, W3Y>;
+  const Tex T{c.s_src, c.sx0, c.sy0, m, c.src};
+  const FastTex FT{c.s_src, W3X, c.sx0, c.sy0, m};
+
+  // velocity at every forward-region texel centre (shared by the +h and -h traces) and
+  // the forward trace from it
+  for (int i = tid; i < W2X * W2Y; i += NT) {
+    const int ry = i / W2X, rx = i - ry * W2X;
+    const float2 p = texel_pos((c.fx0 + rx) & (m - 1), (c.fy0 + ry) & (m - 1), m);
+    const float2 v1 = vel_at(p.x, p.y);
+    c.s_v1[i] = v1;
+    c.s_sp[i] = trace(p.x, p.y, v1, h);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // forward pass over the forward region
+  for (int i = tid; i < W2X * W2Y; i += NT) {
+    const float2 sp = c.s_sp[i];
+    const Footprint f = footprint(sp.x, sp.y, m);
+    Rgb r;
+    if constexpr (FAST) r = FT.sample(f);
+    else r = bilerp_rgb(T, f);
+    c.s_fwd[i] = pack_rgb(r);
+  }
+  __syncthreads();
+
+  using FE = FwdEval<Tex>;
+  using FF = DerivedTex<FE, W2X, W2Y>;
+  const FE fe{V, T, h, n, m};
+  const FF ff{c.s_fwd, c.fx0, c.fy0, m, fe};
+  const FastTex FFT{c.s_fwd, W2X, c.fx0, c.fy0, m};
+  // backward pass over the backward region (nested in the forward region by kDyeLo / kDyeHi)
+  for (int i = tid; i < W1X * W1Y; i += NT) {
+    const int ry = i / W1X, rx = i - ry * W1X;
+    const int fi = (ry + kDyeLo) * W2X + rx + kDyeLo;
+    const float2 p = texel_pos((c.bx0 + rx) & (m - 1), (c.by0 + ry) & (m - 1), m);
+    const float2 sb = trace(p.x, p.y, c.s_v1[fi], -h);
+    const Footprint f = footprint(sb.x, sb.y, m);
+    Rgb r;
+    if constexpr (FAST) r = FFT.sample(f);
+    else r = bilerp_rgb(ff, f);
+    c.s_back[i] = pack_rgb(r);
+  }
+  __syncthreads();
+
+  using BE = BackEval<FF>;
+  const BE be{V, ff, h, n, m};
+  const DerivedTex<BE, W1X, W1Y> bf{c.s_back, c.bx0, c.by0, m, be};
+  const FastTex FB{c.s_back, W1X, c.bx0, c.by0, m};
+  for (int i = tid; i < TX * TY; i += NT) {
+    const int ry = i / TX, rx = i - ry * TX;
+    const int x = c.tx0 + rx, y = c.ty0 + ry;
+    const float2 p = texel_pos(x, y, m);
+    const float2 sp = c.s_sp[(ry + 2 * kDyeLo) * W2X + rx + 2 * kDyeLo];
+    const Footprint f = footprint(sp.x, sp.y, m);
+    Rgb lo, hi, a, b;
+    if constexpr (FAST) {
+      a = FT.sample(f, &lo, &hi);
+      b = FB.sample(f);
+    } else {
+      a = bilerp_rgb(T, f, &lo, &hi);
+      b = bilerp_rgb(bf, f);
+    }
+    c.dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, p.x, p.y, c.fade, c.S);
+  }
+}
+// the general passes kept out of line: the rarely taken path with its recomputation
+// chains does not set the register budget of the fast path
+template <int TX> __device__ __noinline__ void dye_cta_passes_general(const DyeCta<TX>& c) {
+  dye_cta_passes<TX, false>(c);
+}
+
 template <int TX>
 __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
     k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
@@ -432,90 +570,60 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   constexpr int TY = G::TY, NT = G::THREADS;
   constexpr int W1X = G::W1X, W1Y = G::W1Y, W2X = G::W2X, W2Y = G::W2Y, W3X = G::W3X, W3Y = G::W3Y;
   extern __shared__ uint2 dsm2[];
-  uint2* s_src = dsm2;
-  uint2* s_back = s_src + W3X * W3Y;
-  uint2* s_fwd = s_back + W1X * W1Y;
-  float2* s_v1 = reinterpret_cast<float2*>(s_fwd + W2X * W2Y);   // velocity at forward-region texels
-  float2* s_sp = s_v1 + W2X * W2Y;                                // their forward trace positions
-  float2* s_vel = s_sp + W2X * W2Y;
-  const int vwx = G::vel_x(n, m), vwy = G::vel_y(n, m);
-  const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
+  DyeCta<TX> c;
+  c.vel = vel;
+  c.src = src;
+  c.dst = dst;
+  c.S = S;
+  c.s_src = dsm2;
+  c.s_back = c.s_src + W3X * W3Y;
+  c.s_fwd = c.s_back + W1X * W1Y;
+  c.s_v1 = reinterpret_cast<float2*>(c.s_fwd + W2X * W2Y);   // velocity at forward-region texels
+  c.s_sp = c.s_v1 + W2X * W2Y;                                // their forward trace positions
+  c.s_vel = c.s_sp + W2X * W2Y;
+  c.n = n;
+  c.m = m;
+  c.vwx = G::vel_x(n, m);
+  c.vwy = G::vel_y(n, m);
+  c.tx0 = blockIdx.x * TX;
+  c.ty0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
-  const float h = __fdiv_rn(dtbuf[0], kTwoPiF);
+  c.h = __fdiv_rn(dtbuf[0], kTwoPiF);
+  c.fade = params->dye_fade;
 
   // origins (wrapped) of the on-chip windows
-  const int sx0 = (tx0 - 3 * kDyeLo) & (m - 1), sy0 = (ty0 - 3 * kDyeLo) & (m - 1);
-  const int fx0 = (tx0 - 2 * kDyeLo) & (m - 1), fy0 = (ty0 - 2 * kDyeLo) & (m - 1);
-  const int bx0 = (tx0 - kDyeLo) & (m - 1), by0 = (ty0 - kDyeLo) & (m - 1);
-  const int vx0 = (int)floorf(((float)(tx0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
-  const int vy0 = (int)floorf(((float)(ty0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
-  const int vxw = vx0 & (n - 1), vyw = vy0 & (n - 1);
+  c.sx0 = (c.tx0 - 3 * kDyeLo) & (m - 1);
+  c.sy0 = (c.ty0 - 3 * kDyeLo) & (m - 1);
+  c.fx0 = (c.tx0 - 2 * kDyeLo) & (m - 1);
+  c.fy0 = (c.ty0 - 2 * kDyeLo) & (m - 1);
+  c.bx0 = (c.tx0 - kDyeLo) & (m - 1);
+  c.by0 = (c.ty0 - kDyeLo) & (m - 1);
+  const int vx0 = (int)floorf(((float)(c.tx0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  const int vy0 = (int)floorf(((float)(c.ty0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  c.vxw = vx0 & (n - 1);
+  c.vyw = vy0 & (n - 1);
 
-  // the source window arrives asynchronously while the traces below (velocity only) run
+  // the source window arrives asynchronously while the traces (velocity only) run
 #pragma unroll 4
   for (int i = tid; i < W3X * W3Y; i += NT) {
     const int ry = i / W3X, rx = i - ry * W3X;
-    cp_async8(s_src + i, src + (size_t)((sy0 + ry) & (m - 1)) * m + ((sx0 + rx) & (m - 1)));
+    cp_async8(c.s_src + i, src + (size_t)((c.sy0 + ry) & (m - 1)) * m + ((c.sx0 + rx) & (m - 1)));
   }
   cp_async_commit();
+  // the velocity window, and whether any of its values moves a trace a texel or more: a
+  // sample's velocity is a convex combination of window values, so |u| h m < 0.99 and
+  // |v| h m < 0.99 over the window bound every displacement of the tile below one texel
+  const float lim = 0.99f / (fabsf(c.h) * (float)m);
+  bool far = false;
 #pragma unroll 4
-  for (int i = tid; i < vwx * vwy; i += NT) {
-    const int ry = i / vwx, rx = i - ry * vwx;
-    s_vel[i] = __ldg(vel + (size_t)((vyw + ry) & (n - 1)) * n + ((vxw + rx) & (n - 1)));
+  for (int i = tid; i < c.vwx * c.vwy; i += NT) {
+    const int ry = i / c.vwx, rx = i - ry * c.vwx;
+    const float2 v = __ldg(vel + (size_t)((c.vyw + ry) & (n - 1)) * n + ((c.vxw + rx) & (n - 1)));
+    c.s_vel[i] = v;
+    far |= !(fabsf(v.x) < lim && fabsf(v.y) < lim);
   }
-  __syncthreads();
-
-  const SmemVel V{s_vel, vxw, vyw, vwx, vwy, n, vel};
-  using Tex = SmemTex<W3X, W3Y>;
-  const Tex T{s_src, sx0, sy0, m, src};
-  // velocity at every forward-region texel centre (shared by the +h and -h traces) and
-  // the forward trace from it
-  for (int i = tid; i < W2X * W2Y; i += NT) {
-    const int ry = i / W2X, rx = i - ry * W2X;
-    const float2 p = texel_pos((fx0 + rx) & (m - 1), (fy0 + ry) & (m - 1), m);
-    const float2 v1 = sample_vel_win(V, p.x, p.y);
-    s_v1[i] = v1;
-    s_sp[i] = trace_from(WinVel{V}, p.x, p.y, v1, h, n);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-
-  // forward pass over the forward region
-  for (int i = tid; i < W2X * W2Y; i += NT) {
-    const float2 sp = s_sp[i];
-    s_fwd[i] = pack_rgb(bilerp_rgb(T, footprint(sp.x, sp.y, m)));
-  }
-  __syncthreads();
-
-  using FE = FwdEval<Tex>;
-  using FF = DerivedTex<FE, W2X, W2Y>;
-  const FE fe{V, T, h, n, m};
-  const FF ff{s_fwd, fx0, fy0, m, fe};
-  // backward pass over the backward region (nested in the forward region by kDyeLo / kDyeHi)
-  for (int i = tid; i < W1X * W1Y; i += NT) {
-    const int ry = i / W1X, rx = i - ry * W1X;
-    const int fi = (ry + kDyeLo) * W2X + rx + kDyeLo;
-    const float2 p = texel_pos((bx0 + rx) & (m - 1), (by0 + ry) & (m - 1), m);
-    const float2 sb = trace_from(WinVel{V}, p.x, p.y, s_v1[fi], -h, n);
-    s_back[i] = pack_rgb(bilerp_rgb(ff, footprint(sb.x, sb.y, m)));
-  }
-  __syncthreads();
-
-  using BE = BackEval<FF>;
-  const BE be{V, ff, h, n, m};
-  const DerivedTex<BE, W1X, W1Y> bf{s_back, bx0, by0, m, be};
-  const float fade = params->dye_fade;
-  for (int i = tid; i < TX * TY; i += NT) {
-    const int ry = i / TX, rx = i - ry * TX;
-    const int x = tx0 + rx, y = ty0 + ry;
-    const float2 p = texel_pos(x, y, m);
-    const float2 sp = s_sp[(ry + 2 * kDyeLo) * W2X + rx + 2 * kDyeLo];
-    const Footprint f = footprint(sp.x, sp.y, m);
-    Rgb lo, hi;
-    const Rgb a = bilerp_rgb(T, f, &lo, &hi);
-    const Rgb b = bilerp_rgb(bf, f);
-    dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, p.x, p.y, fade, S);
-  }
+  if (__syncthreads_or(far ? 1 : 0)) dye_cta_passes_general<TX>(c);
+  else dye_cta_passes<TX, true>(c);
 }
 
 }  // namespace s2d

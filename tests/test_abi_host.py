@@ -74,6 +74,15 @@ def test_unknown_fft_arithmetic_rejected(pkg):
         pkg.Solver.create(n=64, fft="fp8")
 
 
+@pytest.mark.parametrize("scale", [0, 3, 5, 8])
+def test_dye_scale_must_be_a_power_of_two(pkg, scale):
+    """The dye grid wraps texel indices with a power-of-two mask: dyeScale 1, 2 (the
+    reference's choices, main.js:196) or 4; the check precedes any device work."""
+    with pytest.raises(pkg.S2DError) as ei:
+        pkg.Solver.create(n=64, dyeScale=scale)
+    assert ei.value.status == -1
+
+
 # ---------------------------------------------------------------- WGSL restatement self-checks
 def test_hash_matches_js_imul_semantics():
     # hash32 (solver.js:43-47) written with JS-style 32-bit wrapping in Python ints

@@ -157,8 +157,11 @@ def test_dye_bfecc_step(pkg, m_scale):
 
 @pytest.mark.parametrize("n,m_scale", [(64, 1), (128, 2), (256, 4)])
 def test_fused_dye_equals_three_passes(pkg, n, m_scale):
-    """The one-launch dye step reproduces the reference's three dispatches bit for bit,
-    also when a large fixed dt pushes back-traces past the on-chip halo."""
+    """The one-launch dye step reproduces the reference's three dispatches bit for bit:
+    at the CFL dt (tiles whose traces stay under one texel take the untested window
+    lookups), at a dt moving the fastest traces 1.5 texels (tiles of both kinds in one
+    launch) and at a dt moving them several texels (back-traces past the on-chip halo,
+    recomputed from global memory)."""
     splat = {"x": 0.1, "y": 0.9, "dx": -0.01, "dy": 0.02, "color": (0.36, 0.93, 0.66), "radius": 0.08,
              "amp": 0.0, "dyeAmp": 1.0}
     outs = []
@@ -169,7 +172,10 @@ def test_fused_dye_equals_three_passes(pkg, n, m_scale):
             s.reset({"k0": 8, "amplitude": 10, "seed": 4, "dyePattern": "bands"})
             s.setSplats([splat])
             s.encodePrime()
-            for dt in (None, 0.05):                      # CFL dt, then a step of several texels
+            vel = s.getBuffer("vel")
+            vmax = float(max(np.abs(vel.real).max(), np.abs(vel.imag).max()))
+            dt_mixed = 1.5 * 2 * np.pi / (vmax * n * m_scale)
+            for dt in (None, dt_mixed, 0.05):
                 if dt is not None:
                     set_fixed_dt(s, dt)
                 for _ in range(2):
@@ -177,5 +183,6 @@ def test_fused_dye_equals_three_passes(pkg, n, m_scale):
                 outs.append(s.currentDye)
         finally:
             s.destroy()
-    assert np.array_equal(outs[0], outs[2])
-    assert np.array_equal(outs[1], outs[3])
+    assert np.array_equal(outs[0], outs[3])
+    assert np.array_equal(outs[1], outs[4])
+    assert np.array_equal(outs[2], outs[5])
