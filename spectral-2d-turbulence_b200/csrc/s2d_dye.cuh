@@ -150,16 +150,18 @@ __device__ __forceinline__ Rgba bilerp(const TF& tf, const Footprint& f, Rgba* l
 
 // texel centre (x + 0.5)/m; m is a power of two, so x/m, 0.5/m and their sum (2x+1)/(2m)
 // are all exact and one fused multiply-add gives the quotient
-__device__ __forceinline__ float2 texel_pos(int x, int y, int m) {
-  const float inv = __frcp_rn((float)m);
-  const float half_inv = 0.5f * inv;
-  return make_float2(__fmaf_rn((float)x, inv, half_inv), __fmaf_rn((float)y, inv, half_inv));
+__device__ __forceinline__ float2 texel_pos(int x, int y, float inv_m) {
+  const float half_inv = 0.5f * inv_m;
+  return make_float2(__fmaf_rn((float)x, inv_m, half_inv), __fmaf_rn((float)y, inv_m, half_inv));
 }
+__device__ __forceinline__ float2 texel_pos(int x, int y, int m) { return texel_pos(x, y, __frcp_rn((float)m)); }
 
 // BFECC correction of one texel from its source (a, with the 4-texel min/max) and
-// back-advected (b) samples, fade and splat dye (dye.wgsl:81-112)
-__device__ __forceinline__ uint2 correct_from(const Rgba& a, const Rgba& b, const Rgba& lo, const Rgba& hi, float px,
-                                              float py, float fade, const DevSplats* __restrict__ S) {
+// back-advected (b) samples, fade and splat dye (dye.wgsl:81-112); pos() gives the texel
+// centre, formed only when there are splats to place
+template <class POS>
+__device__ __forceinline__ uint2 correct_from(const Rgba& a, const Rgba& b, const Rgba& lo, const Rgba& hi,
+                                              const POS& pos, float fade, const DevSplats* __restrict__ S) {
   auto corr = [&](float x, float y, float l, float u) {
     return __fmul_rn(fminf(fmaxf(__fsub_rn(__fmul_rn(1.5f, x), __fmul_rn(0.5f, y)), l), u), fade);
   };
@@ -167,6 +169,9 @@ __device__ __forceinline__ uint2 correct_from(const Rgba& a, const Rgba& b, cons
   float g = corr(a.g, b.g, lo.g, hi.g);
   float bb = corr(a.b, b.b, lo.b, hi.b);
   const int cnt = S->count;
+  if (cnt == 0) return pack_texel(r, g, bb, 1.f);
+  const float2 p = pos();
+  const float px = p.x, py = p.y;
   for (int i = 0; i < cnt; ++i) {
     const DevSplat sp = S->items[i];
     const float rx = sepf(px, sp.x), ry = sepf(py, sp.y);
@@ -188,7 +193,7 @@ __device__ __forceinline__ uint2 correct_texel(const SF& src, const BF& back, co
   Rgba lo, hi;
   const Rgba a = bilerp(src, f, &lo, &hi);
   const Rgba b = bilerp(back, f);
-  return correct_from(a, b, lo, hi, px, py, fade, S);
+  return correct_from(a, b, lo, hi, [&] { return make_float2(px, py); }, fade, S);
 }
 
 // ---------------------------------------------------------------- three passes (reference order)
@@ -233,7 +238,10 @@ template <int TX> struct DyeGeom {
   static constexpr int H = kDyeLo + kDyeHi;
   static constexpr int W1X = TX + H, W1Y = TY + H;           // backward-pass region
   static constexpr int W2X = TX + 2 * H, W2Y = TY + 2 * H;   // forward-pass region
-  static constexpr int W3X = TX + 3 * H, W3Y = TY + 3 * H;   // source region
+  // source region, widened by one texel below so that its rows start on an even texel
+  // and arrive in 16-byte copies
+  static constexpr int W3X = TX + 3 * H + 1, W3Y = TY + 3 * H;
+  static_assert(W3X % 2 == 0 && TX % 2 == 0, "16-byte source rows");
   // velocity cells needed by traces from the forward-pass region, for an n x n velocity
   // grid under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation /
   // rounding cells on each side
@@ -252,6 +260,12 @@ inline bool dye_wide_tile(int n, int m) { return m >= 64 && m >= 2 * n; }
 // 8-byte asynchronous global -> shared copy (no register staging) and its wait
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+// 16-byte variant (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
                "l"(src)
                : "memory");
 }
@@ -391,6 +405,18 @@ __device__ __forceinline__ float2 sample_vel(const FastVel& v, float px, float p
   const float2* p = v.sm + (((int)by - v.oy) & (n - 1)) * v.w + (((int)bx - v.ox) & (n - 1));
   return lerp2v(lerp2v(p[0], p[1], fx), lerp2v(p[v.w], p[v.w + 1], fx), fy);
 }
+// velocity at the centre of dye texel (x, y) (wrapped indices) on a dye grid s = m / n
+// times the velocity grid: the centre's velocity coordinate (2x + 1 - s) / (2s) is exact in
+// FP32, so its floor and fraction -- the cell and the weight sample_vel derives from the
+// position -- follow from integer arithmetic (lg2s = log2(2s), inv2s = 1/(2s)), and the
+// lerps see the same operands
+__device__ __forceinline__ float2 vel_centre(const FastVel& v, int x, int y, int s, int lg2s, float inv2s) {
+  const int tx = 2 * x + 1 - s, ty = 2 * y + 1 - s;
+  const float fx = (float)(tx & (2 * s - 1)) * inv2s, fy = (float)(ty & (2 * s - 1)) * inv2s;
+  const int n = v.n;
+  const float2* p = v.sm + (((ty >> lg2s) - v.oy) & (n - 1)) * v.w + (((tx >> lg2s) - v.ox) & (n - 1));
+  return lerp2v(lerp2v(p[0], p[1], fx), lerp2v(p[v.w], p[v.w + 1], fx), fy);
+}
 
 // binary16 W x WY window whose texels outside the window are re-derived by EVAL
 template <class EVAL, int W, int WY>
@@ -446,10 +472,11 @@ struct BackEval {
 };
 
 // BFECC correction from r, g, b (the arithmetic of correct_from; alpha is not read)
-__device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const Rgb& lo, const Rgb& hi, float px,
-                                             float py, float fade, const DevSplats* __restrict__ S) {
+template <class POS>
+__device__ __forceinline__ uint2 correct_rgb(const Rgb& a, const Rgb& b, const Rgb& lo, const Rgb& hi, const POS& pos,
+                                             float fade, const DevSplats* __restrict__ S) {
   const Rgba a4{a.r, a.g, a.b, 1.f}, b4{b.r, b.g, b.b, 1.f}, lo4{lo.r, lo.g, lo.b, 0.f}, hi4{hi.r, hi.g, hi.b, 0.f};
-  return correct_from(a4, b4, lo4, hi4, px, py, fade, S);
+  return correct_from(a4, b4, lo4, hi4, pos, fade, S);
 }
 
 // Windows, origins and constants of one CTA of the fused dye kernel.
@@ -478,11 +505,15 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   const int tid = threadIdx.x;
   const int n = c.n, m = c.m;
   const float h = c.h;
+  const float inv_m = __frcp_rn((float)m);
+  const int s = m / n, lg2s = 31 - __clz(2 * s);
+  const float inv2s = __frcp_rn((float)(2 * s));
   const SmemVel V{c.s_vel, c.vxw, c.vyw, c.vwx, c.vwy, n, c.vel};
   const FastVel FV{c.s_vel, c.vwx, c.vxw, c.vyw, n};
-  auto vel_at = [&](float px, float py) {
-    if constexpr (FAST) return sample_vel(FV, px, py, n);
-    else return sample_vel_win(V, px, py);
+  // velocity at the centre of texel (x, y), at position p
+  auto vel_at = [&](int x, int y, float2 p) {
+    if constexpr (FAST) return vel_centre(FV, x, y, s, lg2s, inv2s);
+    else return sample_vel_win(V, p.x, p.y);
   };
   auto trace = [&](float px, float py, float2 v1, float hs) {
     if constexpr (FAST) return trace_from(FV, px, py, v1, hs, n);
@@ -496,8 +527,9 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   // the forward trace from it
   for (int i = tid; i < W2X * W2Y; i += NT) {
     const int ry = i / W2X, rx = i - ry * W2X;
-    const float2 p = texel_pos((c.fx0 + rx) & (m - 1), (c.fy0 + ry) & (m - 1), m);
-    const float2 v1 = vel_at(p.x, p.y);
+    const int x = (c.fx0 + rx) & (m - 1), y = (c.fy0 + ry) & (m - 1);
+    const float2 p = texel_pos(x, y, inv_m);
+    const float2 v1 = vel_at(x, y, p);
     c.s_v1[i] = v1;
     c.s_sp[i] = trace(p.x, p.y, v1, h);
   }
@@ -524,7 +556,7 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   for (int i = tid; i < W1X * W1Y; i += NT) {
     const int ry = i / W1X, rx = i - ry * W1X;
     const int fi = (ry + kDyeLo) * W2X + rx + kDyeLo;
-    const float2 p = texel_pos((c.bx0 + rx) & (m - 1), (c.by0 + ry) & (m - 1), m);
+    const float2 p = texel_pos((c.bx0 + rx) & (m - 1), (c.by0 + ry) & (m - 1), inv_m);
     const float2 sb = trace(p.x, p.y, c.s_v1[fi], -h);
     const Footprint f = footprint(sb.x, sb.y, m);
     Rgb r;
@@ -541,7 +573,6 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   for (int i = tid; i < TX * TY; i += NT) {
     const int ry = i / TX, rx = i - ry * TX;
     const int x = c.tx0 + rx, y = c.ty0 + ry;
-    const float2 p = texel_pos(x, y, m);
     const float2 sp = c.s_sp[(ry + 2 * kDyeLo) * W2X + rx + 2 * kDyeLo];
     const Footprint f = footprint(sp.x, sp.y, m);
     Rgb lo, hi, a, b;
@@ -552,7 +583,7 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
       a = bilerp_rgb(T, f, &lo, &hi);
       b = bilerp_rgb(bf, f);
     }
-    c.dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, p.x, p.y, c.fade, c.S);
+    c.dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, [&] { return texel_pos(x, y, inv_m); }, c.fade, c.S);
   }
 }
 // the general passes kept out of line: the rarely taken path with its recomputation
@@ -569,7 +600,7 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   using G = DyeGeom<TX>;
   constexpr int TY = G::TY, NT = G::THREADS;
   constexpr int W1X = G::W1X, W1Y = G::W1Y, W2X = G::W2X, W2Y = G::W2Y, W3X = G::W3X, W3Y = G::W3Y;
-  extern __shared__ uint2 dsm2[];
+  extern __shared__ __align__(16) uint2 dsm2[];
   DyeCta<TX> c;
   c.vel = vel;
   c.src = src;
@@ -592,7 +623,7 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   c.fade = params->dye_fade;
 
   // origins (wrapped) of the on-chip windows
-  c.sx0 = (c.tx0 - 3 * kDyeLo) & (m - 1);
+  c.sx0 = (c.tx0 - 3 * kDyeLo - 1) & (m - 1);   // even: rows of 16-byte texel pairs
   c.sy0 = (c.ty0 - 3 * kDyeLo) & (m - 1);
   c.fx0 = (c.tx0 - 2 * kDyeLo) & (m - 1);
   c.fy0 = (c.ty0 - 2 * kDyeLo) & (m - 1);
@@ -603,11 +634,13 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   c.vxw = vx0 & (n - 1);
   c.vyw = vy0 & (n - 1);
 
-  // the source window arrives asynchronously while the traces (velocity only) run
-#pragma unroll 4
-  for (int i = tid; i < W3X * W3Y; i += NT) {
-    const int ry = i / W3X, rx = i - ry * W3X;
-    cp_async8(c.s_src + i, src + (size_t)((c.sy0 + ry) & (m - 1)) * m + ((c.sx0 + rx) & (m - 1)));
+  // the source window arrives asynchronously while the traces (velocity only) run: one
+  // warp per row, a texel pair per 16-byte copy (a pair starts on an even texel, so it
+  // never straddles the periodic seam)
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int ry = warp; ry < W3Y; ry += NT / 32) {
+    const uint2* grow = src + (size_t)((c.sy0 + ry) & (m - 1)) * m;
+    for (int k = lane; k < W3X / 2; k += 32) cp_async16(c.s_src + ry * W3X + 2 * k, grow + ((c.sx0 + 2 * k) & (m - 1)));
   }
   cp_async_commit();
   // the velocity window, and whether any of its values moves a trace a texel or more: a
@@ -615,12 +648,13 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   // |v| h m < 0.99 over the window bound every displacement of the tile below one texel
   const float lim = 0.99f / (fabsf(c.h) * (float)m);
   bool far = false;
-#pragma unroll 4
-  for (int i = tid; i < c.vwx * c.vwy; i += NT) {
-    const int ry = i / c.vwx, rx = i - ry * c.vwx;
-    const float2 v = __ldg(vel + (size_t)((c.vyw + ry) & (n - 1)) * n + ((c.vxw + rx) & (n - 1)));
-    c.s_vel[i] = v;
-    far |= !(fabsf(v.x) < lim && fabsf(v.y) < lim);
+  for (int ry = warp; ry < c.vwy; ry += NT / 32) {
+    const float2* grow = vel + (size_t)((c.vyw + ry) & (n - 1)) * n;
+    for (int rx = lane; rx < c.vwx; rx += 32) {
+      const float2 v = __ldg(grow + ((c.vxw + rx) & (n - 1)));
+      c.s_vel[ry * c.vwx + rx] = v;
+      far |= !(fabsf(v.x) < lim && fabsf(v.y) < lim);
+    }
   }
   if (__syncthreads_or(far ? 1 : 0)) dye_cta_passes_general<TX>(c);
   else dye_cta_passes<TX, true>(c);
