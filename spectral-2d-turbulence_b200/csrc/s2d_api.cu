@@ -133,10 +133,18 @@ struct GraphEntry {
 static size_t diag_block_bytes(int nbins, int n) {
   return (sizeof(double) + sizeof(uint32_t)) * (size_t)(nbins + 2) + sizeof(float) * (size_t)n;
 }
+// the two dt slots follow the diagnostics block in its allocation, so that copyDiagnostics
+// reads both in one copy
+static size_t diag_dt_offset(int nbins, int n) { return (diag_block_bytes(nbins, n) + 15) & ~size_t(15); }
+static size_t diag_alloc_bytes(int nbins, int n) { return diag_dt_offset(nbins, n) + 4 * sizeof(float); }
 
 constexpr int kUploadSlots = 8;
 constexpr size_t kUploadSlotBytes = 512;
-static_assert(sizeof(DevParams) <= kUploadSlotBytes && sizeof(DevSplats) <= kUploadSlotBytes, "upload slot");
+// the parameter and splat blocks sit back to back in one device allocation, so that a
+// configure() and a setSplats() before a step travel in one copy
+constexpr size_t kConstBytes = sizeof(DevParams) + sizeof(DevSplats);
+static_assert(kConstBytes <= kUploadSlotBytes, "upload slot");
+static_assert(sizeof(DevParams) % 16 == 0, "splat block alignment");
 
 struct s2d_solver {
   int dev = 0, n = 0, m = 0, nbins = 0, dye_scale = 1, fft_precision = 0;
@@ -145,13 +153,14 @@ struct s2d_solver {
   float2* state[3] = {nullptr, nullptr, nullptr};
   float2 *packA = nullptr, *packB = nullptr, *physZ = nullptr, *rhs = nullptr, *force = nullptr,
          *vel = nullptr, *tw = nullptr;
-  float* dtbuf = nullptr;      // 2 slots x [dt, speed]
+  float* dtbuf = nullptr;      // 2 slots x [dt, speed], inside diag's allocation
   float* partials = nullptr;
   unsigned* ticket = nullptr;
   DevParams* dparams = nullptr;
-  DevSplats* dsplats = nullptr;
+  DevSplats* dsplats = nullptr;   // inside dparams' allocation, right after the parameters
   // diagnostics block, one allocation (one clear, one readback copy): FP64 bins + totals
-  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n]
+  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n], then (16-byte
+  // aligned) the dt slots
   double* diag = nullptr;
   uint32_t* diag_fixed = nullptr;   // inside diag's allocation
   float* zonal = nullptr;           // inside diag's allocation
@@ -168,7 +177,8 @@ struct s2d_solver {
   double* h_diag = nullptr;
   uint32_t* h_fixed = nullptr;      // inside h_diag's allocation
   float* h_zonal = nullptr;         // inside h_diag's allocation
-  float* h_dt = nullptr;
+  float* h_dt = nullptr;            // inside h_diag's allocation: both dt slots
+  int h_dt_slot = 0;                // the slot current when the copy was enqueued
   cudaEvent_t diag_event = nullptr;
   // pinned upload ring for the per-step parameter and splat blocks: slot i is rewritten
   // only after the copy that last read it has run (upload_ev[i])
@@ -179,6 +189,8 @@ struct s2d_solver {
   DevParams hp{};
   DevSplats hs{};
   bool configured = false;
+  // host blocks changed since their last upload (sent together before the next device work)
+  bool params_dirty = false, splats_dirty = false;
   int phase = 0, dye_parity = 0, slot = 0;
   uint32_t step_index = 0;
   double sim_time = 0.0;
@@ -262,11 +274,11 @@ static void free_solver(s2d_solver* s) {
   }
   s->prof_events.clear();
   void* dev_ptrs[] = {s->state[0], s->state[1], s->state[2], s->packA, s->packB, s->physZ, s->rhs,
-                      s->force, s->vel, s->tw, s->dtbuf, s->partials, s->ticket, s->dparams, s->dsplats,
-                      s->diag, s->seed_parts, s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
+                      s->force, s->vel, s->tw, s->partials, s->ticket, s->dparams, s->diag, s->seed_parts,
+                      s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
-  void* host_ptrs[] = {s->h_diag, s->h_dt, s->h_upload};
+  void* host_ptrs[] = {s->h_diag, s->h_upload};
   for (void* p : host_ptrs)
     if (p) cudaFreeHost(p);
   if (s->diag_event) cudaEventDestroy(s->diag_event);
@@ -289,10 +301,32 @@ static cudaError_t upload(s2d_solver* s, void* dst, const void* src, size_t byte
   return cudaEventRecord(s->upload_ev[i], s->stream);
 }
 
-#define S2D_USE(s)                                                         \
+// configure() and setSplats() only update the host blocks; the changed ones go to the
+// device in one copy ahead of the next call that enqueues work or reads the device
+// (every entry point below except those two and the host-only getters)
+static int flush_uploads(s2d_solver* s) {
+  if (!s->params_dirty && !s->splats_dirty) return S2D_OK;
+  DeviceGuard guard(s->dev);
+  char block[kConstBytes];
+  std::memcpy(block, &s->hp, sizeof(DevParams));
+  std::memcpy(block + sizeof(DevParams), &s->hs, sizeof(DevSplats));
+  const size_t lo = s->params_dirty ? 0 : sizeof(DevParams);
+  const size_t hi = s->splats_dirty ? kConstBytes : sizeof(DevParams);
+  const cudaError_t e = upload(s, reinterpret_cast<char*>(s->dparams) + lo, block + lo, hi - lo);
+  if (e != cudaSuccess) return fail(S2D_ERR_CUDA, std::string("parameter upload: ") + cudaGetErrorString(e));
+  s->params_dirty = s->splats_dirty = false;
+  return S2D_OK;
+}
+
+#define S2D_USE_HOST(s)                                                    \
   do {                                                                     \
     if (!(s)) return fail(S2D_ERR_ARG, "null solver handle");              \
     if ((s)->disposed) return fail(S2D_ERR_DESTROYED, "solver destroyed"); \
+  } while (0)
+#define S2D_USE(s)                                   \
+  do {                                               \
+    S2D_USE_HOST(s);                                 \
+    if (int rc_ = flush_uploads(s)) return rc_;      \
   } while (0)
 
 // ------------------------------------------------------------------ library entry points
@@ -500,27 +534,27 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMalloc(&s->force, cbytes), "force");
   TRY(cudaMalloc(&s->vel, cbytes), "vel");
   TRY(cudaMalloc(&s->tw, sizeof(float2) * n), "twiddles");
-  TRY(cudaMalloc(&s->dtbuf, sizeof(float) * 4), "dt");
   // column-kernel grids are at most n CTAs in every registered shape
   const int nparts = std::max(std::max(n, 256), seed_parts_count(n));
   TRY(cudaMalloc(&s->partials, sizeof(float) * nparts), "partials");
   TRY(cudaMalloc(&s->ticket, sizeof(unsigned)), "ticket");
   TRY(cudaMalloc(&s->row_nz, sizeof(int) * n), "row flags");
-  TRY(cudaMalloc(&s->dparams, sizeof(DevParams)), "params");
-  TRY(cudaMalloc(&s->dsplats, sizeof(DevSplats)), "splats");
-  TRY(cudaMalloc(&s->diag, diag_block_bytes(s->nbins, n)), "diag");
+  TRY(cudaMalloc(&s->dparams, kConstBytes), "params");
+  s->dsplats = reinterpret_cast<DevSplats*>(reinterpret_cast<char*>(s->dparams) + sizeof(DevParams));
+  TRY(cudaMalloc(&s->diag, diag_alloc_bytes(s->nbins, n)), "diag");
   s->diag_fixed = reinterpret_cast<uint32_t*>(s->diag + s->nbins + 2);
   s->zonal = reinterpret_cast<float*>(s->diag_fixed + s->nbins + 2);
+  s->dtbuf = reinterpret_cast<float*>(reinterpret_cast<char*>(s->diag) + diag_dt_offset(s->nbins, n));
   TRY(cudaMalloc(&s->seed_parts, sizeof(double) * seed_parts_count(n)), "seed partials");
   TRY(cudaMalloc(&s->step_counter, sizeof(uint32_t)), "step counter");
   TRY(cudaMalloc(&s->err, sizeof(int)), "error word");
   TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream), "memset");
   TRY(cudaMemsetAsync(s->step_counter, 0, sizeof(uint32_t), s->stream), "memset");
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
-  TRY(cudaMallocHost(&s->h_diag, diag_block_bytes(s->nbins, n)), "pinned diag");
+  TRY(cudaMallocHost(&s->h_diag, diag_alloc_bytes(s->nbins, n)), "pinned diag");
   s->h_fixed = reinterpret_cast<uint32_t*>(s->h_diag + s->nbins + 2);
   s->h_zonal = reinterpret_cast<float*>(s->h_fixed + s->nbins + 2);
-  TRY(cudaMallocHost(&s->h_dt, sizeof(float) * 4), "pinned dt");
+  s->h_dt = reinterpret_cast<float*>(reinterpret_cast<char*>(s->h_diag) + diag_dt_offset(s->nbins, n));
   TRY(cudaMallocHost(&s->h_upload, kUploadSlotBytes * kUploadSlots), "pinned upload ring");
   for (cudaEvent_t& ev : s->upload_ev) TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
   TRY(set_all_attrs(*ops), "kernel attributes");
@@ -564,8 +598,12 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   s->hp.force_norm = (float)(0.01 * n * n);
   s->hp.dx = (float)(2.0 * M_PI / n);
   s->hs = DevSplats{};
-  TRY(upload(s, s->dparams, &s->hp, sizeof(DevParams)), "params");
-  TRY(upload(s, s->dsplats, &s->hs, sizeof(DevSplats)), "splats");
+  s->params_dirty = s->splats_dirty = true;
+  if (int rc = flush_uploads(s)) {
+    free_solver(s);
+    delete s;
+    return rc;
+  }
   TRY(cudaStreamSynchronize(s->stream), "create sync");
 #undef TRY
   *out = s;
@@ -583,7 +621,7 @@ extern "C" int s2d_destroy(s2d_solver* s) {
 }
 
 extern "C" int s2d_get_info(s2d_solver* s, s2d_info* out) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   if (!out) return fail(S2D_ERR_ARG, "out is null");
   out->n = s->n;
   out->m = s->m;
@@ -599,7 +637,7 @@ extern "C" int s2d_get_info(s2d_solver* s, s2d_info* out) {
 }
 
 extern "C" int s2d_set_phase(s2d_solver* s, int phase, int dye_parity) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   if (phase < 0 || phase > 2 || dye_parity < 0 || dye_parity > 1) return fail(S2D_ERR_ARG, "phase out of range");
   if (phase != s->phase) s->packs_valid = false;
   s->phase = phase;
@@ -608,13 +646,13 @@ extern "C" int s2d_set_phase(s2d_solver* s, int phase, int dye_parity) {
 }
 
 extern "C" int s2d_set_sim_time(s2d_solver* s, double t) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   s->sim_time = t;
   return S2D_OK;
 }
 
 extern "C" int s2d_get_stream(s2d_solver* s, void** stream) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   if (!stream) return fail(S2D_ERR_ARG, "out is null");
   *stream = (void*)s->stream;
   return S2D_OK;
@@ -666,10 +704,9 @@ extern "C" int s2d_synchronize(s2d_solver* s) {
 
 // ------------------------------------------------------------------ parameters
 extern "C" int s2d_configure(s2d_solver* s, const s2d_params* p) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   if (!p) return fail(S2D_ERR_ARG, "params is null");
   if (p->hyper_p < 0 || p->hyper_p > 16) return fail(S2D_ERR_ARG, "hyperP must be in 0..16");
-  DeviceGuard guard(s->dev);
   const double kcut = s->n / 3.0;
   DevParams& h = s->hp;
   h.beta = p->beta;
@@ -688,15 +725,14 @@ extern "C" int s2d_configure(s2d_solver* s, const s2d_params* p) {
   h.kcut = (float)kcut;
   h.force_norm = (float)(0.01 * s->n * s->n);
   h.n = s->n;
-  S2D_CUDA(upload(s, s->dparams, &h, sizeof(DevParams)));
+  s->params_dirty = true;   // uploaded with the next device work (flush_uploads)
   s->configured = true;
   return S2D_OK;
 }
 
 extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
-  S2D_USE(s);
+  S2D_USE_HOST(s);
   if (count < 0 || (count > 0 && !list)) return fail(S2D_ERR_ARG, "bad splat list");
-  DeviceGuard guard(s->dev);
   const int c = count < S2D_MAX_SPLATS ? count : S2D_MAX_SPLATS;   // Math.min (solver.js:327)
   s->hs = DevSplats{};
   s->hs.count = c;
@@ -707,7 +743,7 @@ extern "C" int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count) {
     d.r = a.color[0]; d.g = a.color[1]; d.b = a.color[2];
     d.radius = a.radius; d.amp = a.amp; d.dye_amp = a.dye_amp;
   }
-  S2D_CUDA(upload(s, s->dsplats, &s->hs, sizeof(DevSplats)));
+  s->splats_dirty = true;   // uploaded with the next device work (flush_uploads)
   return S2D_OK;
 }
 
@@ -1097,9 +1133,10 @@ extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
   S2D_USE(s);
   if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
   DeviceGuard guard(s->dev);
-  const int nb = s->nbins;
-  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, diag_block_bytes(nb, s->n), cudaMemcpyDeviceToHost, s->stream));
-  S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), sizeof(float) * 2, cudaMemcpyDeviceToHost, s->stream));
+  // the diagnostics block and both dt slots in one copy; the slot current now is the one read
+  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, diag_alloc_bytes(s->nbins, s->n), cudaMemcpyDeviceToHost,
+                           s->stream));
+  s->h_dt_slot = s->slot;
   S2D_CUDA(cudaEventRecord(s->diag_event, s->stream));
   s->read_state = 1;
   return S2D_OK;
@@ -1124,8 +1161,8 @@ extern "C" int s2d_read_diagnostics(s2d_solver* s, double* spectrum, float* zona
   if (zonal) std::memcpy(zonal, s->h_zonal, sizeof(float) * s->n);
   if (energy) *energy = s->h_diag[nb];
   if (enstrophy) *enstrophy = s->h_diag[nb + 1];
-  if (dt) *dt = s->h_dt[0];
-  if (max_speed) *max_speed = s->h_dt[1];
+  if (dt) *dt = s->h_dt[2 * s->h_dt_slot];
+  if (max_speed) *max_speed = s->h_dt[2 * s->h_dt_slot + 1];
   return S2D_OK;
 }
 

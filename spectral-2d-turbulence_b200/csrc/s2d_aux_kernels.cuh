@@ -325,7 +325,9 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
       const double z = 0.5 * ((double)a.x * a.x + (double)a.y * a.y) * inv_n4;
       ens += z;
       if (k2i > 0) {
-        const double e = z / (double)k2i;
+        // z / k2 as z times the correctly rounded reciprocal: within 1.5 ulp of the
+        // quotient, far inside the 1e-12 the FP64 diagnostics are held to
+        const double e = z * __drcp_rn((double)k2i);
         ene += e;
         int b = fb_raw;
         if (b * b - b >= k2i) --b;

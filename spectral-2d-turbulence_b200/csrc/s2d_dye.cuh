@@ -586,19 +586,14 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
     c.dst[(size_t)y * m + x] = correct_rgb(a, b, lo, hi, [&] { return texel_pos(x, y, inv_m); }, c.fade, c.S);
   }
 }
-// the general passes kept out of line: the rarely taken path with its recomputation
-// chains does not set the register budget of the fast path
-template <int TX> __device__ __noinline__ void dye_cta_passes_general(const DyeCta<TX>& c) {
-  dye_cta_passes<TX, false>(c);
-}
-
+// the context of this CTA from the kernel arguments
 template <int TX>
-__global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
-    k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
-                const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
-                const DevSplats* __restrict__ S, int n, int m) {
+__device__ __forceinline__ DyeCta<TX> dye_cta_setup(const float2* __restrict__ vel, const uint2* __restrict__ src,
+                                                    uint2* __restrict__ dst, const float* __restrict__ dtbuf,
+                                                    const DevParams* __restrict__ params,
+                                                    const DevSplats* __restrict__ S, int n, int m) {
   using G = DyeGeom<TX>;
-  constexpr int TY = G::TY, NT = G::THREADS;
+  constexpr int TY = G::TY;
   constexpr int W1X = G::W1X, W1Y = G::W1Y, W2X = G::W2X, W2Y = G::W2Y, W3X = G::W3X, W3Y = G::W3Y;
   extern __shared__ __align__(16) uint2 dsm2[];
   DyeCta<TX> c;
@@ -618,10 +613,8 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   c.vwy = G::vel_y(n, m);
   c.tx0 = blockIdx.x * TX;
   c.ty0 = blockIdx.y * TY;
-  const int tid = threadIdx.x;
   c.h = __fdiv_rn(dtbuf[0], kTwoPiF);
   c.fade = params->dye_fade;
-
   // origins (wrapped) of the on-chip windows
   c.sx0 = (c.tx0 - 3 * kDyeLo - 1) & (m - 1);   // even: rows of 16-byte texel pairs
   c.sy0 = (c.ty0 - 3 * kDyeLo) & (m - 1);
@@ -633,6 +626,28 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   const int vy0 = (int)floorf(((float)(c.ty0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
   c.vxw = vx0 & (n - 1);
   c.vyw = vy0 & (n - 1);
+  return c;
+}
+
+// the general passes kept out of line, from the kernel arguments: the rarely taken path
+// with its recomputation chains neither sets the register budget of the fast path nor
+// makes it keep its context in memory
+template <int TX>
+__device__ __noinline__ void dye_cta_passes_general(const float2* vel, const uint2* src, uint2* dst,
+                                                    const float* dtbuf, const DevParams* params,
+                                                    const DevSplats* S, int n, int m) {
+  dye_cta_passes<TX, false>(dye_cta_setup<TX>(vel, src, dst, dtbuf, params, S, n, m));
+}
+
+template <int TX>
+__global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
+    k_dye_fused(const float2* __restrict__ vel, const uint2* __restrict__ src, uint2* __restrict__ dst,
+                const float* __restrict__ dtbuf, const DevParams* __restrict__ params,
+                const DevSplats* __restrict__ S, int n, int m) {
+  using G = DyeGeom<TX>;
+  constexpr int NT = G::THREADS, W3X = G::W3X, W3Y = G::W3Y;
+  const DyeCta<TX> c = dye_cta_setup<TX>(vel, src, dst, dtbuf, params, S, n, m);
+  const int tid = threadIdx.x;
 
   // the source window arrives asynchronously while the traces (velocity only) run: one
   // warp per row, a texel pair per 16-byte copy (a pair starts on an even texel, so it
@@ -656,7 +671,7 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
       far |= !(fabsf(v.x) < lim && fabsf(v.y) < lim);
     }
   }
-  if (__syncthreads_or(far ? 1 : 0)) dye_cta_passes_general<TX>(c);
+  if (__syncthreads_or(far ? 1 : 0)) dye_cta_passes_general<TX>(vel, src, dst, dtbuf, params, S, n, m);
   else dye_cta_passes<TX, true>(c);
 }
 
