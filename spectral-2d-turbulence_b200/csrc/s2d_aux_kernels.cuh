@@ -229,8 +229,10 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 // memory once per CTA (18.5 -> 14.4 us at 1024^2 against one shared FP64 array whose
 // words the 8 threads of a tile row hit together).  The u32 fixed-point bins use one
 // shared array: the u32 sums wrap
-// mod 2^32 in any order, so the result equals per-cell atomics bit for bit.  CTAs past
-// the tiles take the zonal mean, one warp per two rows.
+// mod 2^32 in any order, so the result equals per-cell atomics bit for bit.  The first
+// CTAs take the zonal mean, one warp per two rows, issuing a lane's loads eight at a time
+// (with one load in flight per lane they took 6.2 us alone at 1024^2); with them the
+// 512 tile CTAs of 1024^2 still fit one wave at 4 CTAs per SM.
 //
 // Per cell: the f32 bin round(sqrtf(k2)) is the reference's; the FP64 bin
 // floor(sqrt(k2) + 0.5) is the same integer corrected by one step with integer tests
@@ -256,25 +258,34 @@ __device__ __forceinline__ int diag_min_abs_wn(int i0, int len, int n) {
 }
 __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, const float2* __restrict__ vel,
                                                   double* out, uint32_t* bins, float* zonal, int n) {
-  const int tiles = diag_tiles(n);
-  if ((int)blockIdx.x >= tiles) {   // zonal mean of u, FP64 accumulation
+  const int zctas = diag_zonal_ctas(n);
+  if ((int)blockIdx.x < zctas) {   // zonal mean of u, FP64 accumulation, one warp per two rows
     const int lane = threadIdx.x & 31;
+    const int nq = n / 2;   // float4 (two velocity cells) per row
 #pragma unroll 1
     for (int r = 0; r < 2; ++r) {
-      const int row = ((int)blockIdx.x - tiles) * 16 + (int)(threadIdx.x >> 5) * 2 + r;
+      const int row = (int)blockIdx.x * 16 + (int)(threadIdx.x >> 5) * 2 + r;
       if (row >= n) return;
       const float4* r4 = reinterpret_cast<const float4*>(vel + (size_t)row * n);
       double acc = 0.0;
-      for (int i = lane; i < n / 2; i += 32) {
-        const float4 t = r4[i];
-        acc += (double)t.x;
-        acc += (double)t.z;
+      // lane order i = lane + 32 j, as one load at a time would sum them
+      for (int base = lane; base < nq; base += 32 * 8) {
+        float4 t[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) t[j] = base + 32 * j < nq ? r4[base + 32 * j] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (base + 32 * j < nq) {
+            acc += (double)t[j].x;
+            acc += (double)t[j].z;
+          }
       }
       acc = warp_sum(acc);
       if (lane == 0) zonal[row] = (float)(acc / n);
     }
     return;
   }
+  const int tile = (int)blockIdx.x - zctas;
   extern __shared__ double win[];                      // [32 lanes][kDiagStride], then 2 totals
   double* const tot = win + 32 * kDiagStride;
   uint32_t* const fhist = reinterpret_cast<uint32_t*>(tot + 2);
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, 
   for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) fhist[i] = 0u;
   const int tw = diag_tile_w(n), th = diag_tile_h(n), per_row = tw / kDiagCells;
   const int tiles_x = n / tw;
-  const int col0 = ((int)blockIdx.x % tiles_x) * tw, row0 = ((int)blockIdx.x / tiles_x) * th;
+  const int col0 = (tile % tiles_x) * tw, row0 = (tile / tiles_x) * th;
   // lowest bin of the tile, less one for rounding: floor(sqrt(min k2)) - 1, and at most
   // the last bin (|k| beyond n/2 is binned there)
   const int mkx = diag_min_abs_wn(col0, tw, n), mky = diag_min_abs_wn(row0, th, n);
