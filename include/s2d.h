@@ -146,6 +146,13 @@ int s2d_synchronize(s2d_solver* s);
 int s2d_probe_wait_timeout(s2d_solver* s, unsigned long long limit_ns);
 
 /* ---------------------------------------------------------------- parameters */
+/* Both update the solver's host copy of the parameter / splat block and return; the
+ * blocks that changed reach the device together, in one copy from pinned memory, at the
+ * start of the next call that enqueues device work or reads the device (every s2d_*
+ * call on the solver except these two, s2d_get_info, s2d_set_phase, s2d_set_sim_time and
+ * s2d_get_stream) -- in stream order before that call's work, as the reference's
+ * writeBuffer precedes the passes encoded after it.  Work a caller enqueues on the
+ * solver's stream directly sees the blocks after the next such call. */
 int s2d_configure(s2d_solver* s, const s2d_params* p);                   /* solver.js:306-324 */
 int s2d_set_splats(s2d_solver* s, const s2d_splat* list, int count);     /* solver.js:326-345 */
 
