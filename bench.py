@@ -277,11 +277,14 @@ def shard_by_cost(instances, world):
 
 # ------------------------------------------------------------------ CPU reference arm
 def _oracle_worker(args):
-    """Run `steps` oracle RK3 steps on the workload; returns (steps, seconds).
+    """Run `steps` oracle steps of the workload -- an RK3 step with forcing and the CFL dt,
+    then the BFECC dye step on the (N * DYE_SCALE)^2 dye with that step's velocity, as the
+    GPU arm's step does -- and return (steps, seconds).
 
     The initial field is `w0` when given (the GPU arm's own initial state, read back from
     the device), else the CPU restatement of the device band seed s2d_seed_band with the
-    GPU arm's seed (1 + rank), so both arms start from the same FP32 field."""
+    GPU arm's seed (1 + rank), so both arms start from the same FP32 field; the dye starts
+    as the 'bands' pattern, as the GPU arm's reset paints it."""
     n, steps, seed, w0 = args
     import numpy as np
     from oracle import wgsl_oracle as wo
@@ -293,24 +296,29 @@ def _oracle_worker(args):
     s.w = np.asarray(init).astype(np.complex128)
     s.step(dt=CFG["dtMax"])        # warm-up
     s.w = np.asarray(init).astype(np.complex128)
+    dye = wo.paint_dye_bands(n * DYE_SCALE)
     t0 = time.perf_counter()
     for k in range(steps):
         dt = s.timestep()
         f = wo.stochastic_forcing(n, CFG["forceAmp"], CFG["forceK"], CFG["forceWidth"], k, dt)
         s.step(dt=dt, forcing=f.astype(np.complex128))
+        u, v = s.velocity()
+        dye = wo.dye_step(dye, np.stack([u, v], axis=-1).astype(np.float32), dt, CFG["dyeFade"])
     return steps, time.perf_counter() - t0
 
 
 def cpu_baseline(w0, budget_s=15.0):
-    """The FP64 NumPy restatement of reference/spectral2d.py, one core, bounded sample,
-    started from the GPU arm's own initial field `w0` (the same FP32 bits)."""
+    """The FP64 NumPy restatement of reference/spectral2d.py plus the FP32 restatement of
+    the dye shader, one core, bounded sample, started from the GPU arm's own initial field
+    `w0` (the same FP32 bits)."""
     steps1, t1 = _oracle_worker((N, 1, 1, w0))
     k = max(1, min(20, int(budget_s / max(t1, 1e-3))))
     steps, secs = _oracle_worker((N, k, 1, w0))
     return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} RK3 steps of one {N}^2 instance with forcing and CFL dt "
-                      f"(FP64 NumPy restatement of reference/spectral2d.py, no dye), {secs:.1f} s; "
-                      "initial field = the GPU arm's seeded state read back from the device (same FP32 bits)"}
+            "sample": f"{steps} steps of one {N}^2 instance: RK3 with forcing and CFL dt (FP64 NumPy "
+                      f"restatement of reference/spectral2d.py) and the BFECC dye step on the "
+                      f"{N * DYE_SCALE}^2 dye (NumPy restatement of dye.wgsl), {secs:.1f} s; initial field = "
+                      "the GPU arm's seeded state read back from the device (same FP32 bits)"}
 
 
 def run_reference(args):
@@ -334,10 +342,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / per,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": N, "replicas": procs},
+        "config": {"workload": WORKLOAD, "n": N, "dye": N * DYE_SCALE, "replicas": procs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
-                         "sample": f"{procs} processes x {per} RK3 steps at {N}^2 (NumPy FP64 restatement of "
-                                   f"reference/spectral2d.py; wall {wall:.1f} s)"},
+                         "sample": f"{procs} processes x {per} steps at {N}^2, each an RK3 step (NumPy FP64 "
+                                   f"restatement of reference/spectral2d.py) and a BFECC dye step on the "
+                                   f"{N * DYE_SCALE}^2 dye (NumPy restatement of dye.wgsl); wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
