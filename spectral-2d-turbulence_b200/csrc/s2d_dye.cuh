@@ -247,11 +247,11 @@ template <int TX> struct DyeGeom {
   // rounding cells on each side
   __host__ __device__ static constexpr int vel_x(int n, int m) { return (W2X + 2) * n / m + 4; }
   __host__ __device__ static constexpr int vel_y(int n, int m) { return (W2Y + 2) * n / m + 4; }
-  // binary16 source / backward / forward windows; FP32 centre velocities and forward
-  // trace positions of the forward region; the velocity window
+  // binary16 source / backward / forward windows; FP32 centre velocities of the forward
+  // region, forward trace positions of the tile; the velocity window
   __host__ __device__ static constexpr size_t smem(int n, int m) {
     return sizeof(uint2) * (W3X * W3Y + W1X * W1Y + W2X * W2Y) +
-           sizeof(float2) * (2 * W2X * W2Y + vel_x(n, m) * vel_y(n, m));
+           sizeof(float2) * (W2X * W2Y + TX * TY + vel_x(n, m) * vel_y(n, m));
   }
 };
 // the wide tile for dye grids at least 2x the velocity grid and 64 texels wide
@@ -523,22 +523,19 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   const Tex T{c.s_src, c.sx0, c.sy0, m, c.src};
   const FastTex FT{c.s_src, W3X, c.sx0, c.sy0, m};
 
-  // velocity at every forward-region texel centre (shared by the +h and -h traces) and
-  // the forward trace from it
+  // forward pass over the forward region (the source window is complete: the caller
+  // waited for its copies before its barrier): the velocity at each texel centre (kept
+  // for the -h trace), the forward trace from it -- kept for the tile's own texels, whose
+  // corrected samples use it -- and the forward-pass texel it samples
   for (int i = tid; i < W2X * W2Y; i += NT) {
     const int ry = i / W2X, rx = i - ry * W2X;
     const int x = (c.fx0 + rx) & (m - 1), y = (c.fy0 + ry) & (m - 1);
     const float2 p = texel_pos(x, y, inv_m);
     const float2 v1 = vel_at(x, y, p);
     c.s_v1[i] = v1;
-    c.s_sp[i] = trace(p.x, p.y, v1, h);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-
-  // forward pass over the forward region
-  for (int i = tid; i < W2X * W2Y; i += NT) {
-    const float2 sp = c.s_sp[i];
+    const float2 sp = trace(p.x, p.y, v1, h);
+    const int ix = rx - 2 * kDyeLo, iy = ry - 2 * kDyeLo;
+    if ((unsigned)ix < (unsigned)TX && (unsigned)iy < (unsigned)TY) c.s_sp[iy * TX + ix] = sp;
     const Footprint f = footprint(sp.x, sp.y, m);
     Rgb r;
     if constexpr (FAST) r = FT.sample(f);
@@ -573,7 +570,7 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
   for (int i = tid; i < TX * TY; i += NT) {
     const int ry = i / TX, rx = i - ry * TX;
     const int x = c.tx0 + rx, y = c.ty0 + ry;
-    const float2 sp = c.s_sp[(ry + 2 * kDyeLo) * W2X + rx + 2 * kDyeLo];
+    const float2 sp = c.s_sp[i];
     const Footprint f = footprint(sp.x, sp.y, m);
     Rgb lo, hi, a, b;
     if constexpr (FAST) {
@@ -605,8 +602,8 @@ __device__ __forceinline__ DyeCta<TX> dye_cta_setup(const float2* __restrict__ v
   c.s_back = c.s_src + W3X * W3Y;
   c.s_fwd = c.s_back + W1X * W1Y;
   c.s_v1 = reinterpret_cast<float2*>(c.s_fwd + W2X * W2Y);   // velocity at forward-region texels
-  c.s_sp = c.s_v1 + W2X * W2Y;                                // their forward trace positions
-  c.s_vel = c.s_sp + W2X * W2Y;
+  c.s_sp = c.s_v1 + W2X * W2Y;                                // forward trace positions of the tile
+  c.s_vel = c.s_sp + TX * TY;
   c.n = n;
   c.m = m;
   c.vwx = G::vel_x(n, m);
@@ -649,7 +646,7 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
   const DyeCta<TX> c = dye_cta_setup<TX>(vel, src, dst, dtbuf, params, S, n, m);
   const int tid = threadIdx.x;
 
-  // the source window arrives asynchronously while the traces (velocity only) run: one
+  // the source window arrives asynchronously while the velocity window loads: one
   // warp per row, a texel pair per 16-byte copy (a pair starts on an even texel, so it
   // never straddles the periodic seam)
   const int warp = tid >> 5, lane = tid & 31;
@@ -671,6 +668,8 @@ __global__ void __launch_bounds__(DyeGeom<TX>::THREADS, DyeGeom<TX>::MINB)
       far |= !(fabsf(v.x) < lim && fabsf(v.y) < lim);
     }
   }
+  // this thread's source copies have landed; the barrier below makes every thread's visible
+  cp_async_wait_all();
   if (__syncthreads_or(far ? 1 : 0)) dye_cta_passes_general<TX>(vel, src, dst, dtbuf, params, S, n, m);
   else dye_cta_passes<TX, true>(c);
 }
