@@ -12,11 +12,11 @@
 //     or 32 when the dye is not refined over the flow) and keeps, in shared memory,
 //     the source texels of the tile plus a 3-level halo, the forward-pass texels of
 //     the tile plus 2 levels and the backward-pass texels plus 1 level; each level's
-//     halo (1 texel below, 2 above) covers the bilinear footprint of a back-trace of
-//     up to one texel, which the CFL limit gives at dyeScale 2.  A sample outside the
-//     on-chip region is recomputed from global memory (the forward/backward values at
-//     that texel are re-derived), so the result does not depend on the halo being
-//     large enough.  Texture traffic drops from 7 texture passes to one read and one
+//     halo (1 texel on each side) covers the bilinear footprint of a trace shorter than
+//     one texel, which the CFL limit gives at dyeScale 2 away from the fastest flow.  A
+//     sample outside the on-chip region is recomputed from global memory (the
+//     forward/backward values at that texel are re-derived), so the result does not
+//     depend on the halo being large enough.  Texture traffic drops from 7 texture passes to one read and one
 //     write.  The source, forward and backward windows hold binary16 texels, as those
 //     textures would (exact), and only r, g, b are carried: the corrected texel's
 //     alpha is 1 whatever the inputs.
@@ -223,13 +223,14 @@ __global__ void k_dye_correct(const float2* __restrict__ vel, const uint2* __res
 }
 
 // ---------------------------------------------------------------- fused single pass
-// Halo per level: a sample displaced by at most one texel from texel x has the bilinear
-// footprint [x - 1, x + 2], so each level extends the region below by 1 and above by 2.
-constexpr int kDyeLo = 1, kDyeHi = 2;
+// Halo per level: a sample displaced by less than one texel from the centre of texel x
+// (floor(x + d) is x - 1 or x for |d| < 1) has the bilinear footprint [x - 1, x + 1], so
+// each level extends the region by one texel on each side.
+constexpr int kDyeLo = 1, kDyeHi = 1;
 constexpr int kDyeTileY = 32;
-// Output tile TX x 32 (TX = 64 when the dye is refined over the flow: 112 KB of windows,
-// 2 CTAs of 512 threads per SM, and 30 % / 15 % of recomputed forward / backward halo
-// texels instead of 41 % / 20 % at TX = 32; TX = 32 otherwise, where the velocity window
+// Output tile TX x 32 (TX = 64 when the dye is refined over the flow: 103 KB of windows,
+// 2 CTAs of 512 threads per SM, and 20 % / 10 % of recomputed forward / backward halo
+// texels instead of 28 % / 14 % at TX = 32; TX = 32 otherwise, where the velocity window
 // is as large as the dye windows)
 template <int TX> struct DyeGeom {
   static constexpr int TY = kDyeTileY;
@@ -238,9 +239,9 @@ template <int TX> struct DyeGeom {
   static constexpr int H = kDyeLo + kDyeHi;
   static constexpr int W1X = TX + H, W1Y = TY + H;           // backward-pass region
   static constexpr int W2X = TX + 2 * H, W2Y = TY + 2 * H;   // forward-pass region
-  // source region, widened by one texel below so that its rows start on an even texel
-  // and arrive in 16-byte copies
-  static constexpr int W3X = TX + 3 * H + 1, W3Y = TY + 3 * H;
+  // source region, widened by one texel below (and one above, for an even width) so that
+  // its rows start on an even texel and arrive in 16-byte copies
+  static constexpr int W3X = (TX + 3 * H + 2) & ~1, W3Y = TY + 3 * H;
   static_assert(W3X % 2 == 0 && TX % 2 == 0, "16-byte source rows");
   // velocity cells needed by traces from the forward-pass region, for an n x n velocity
   // grid under an m x m dye grid: (W2 + 2 displacement texels) * n/m + 2 interpolation /
