@@ -16,10 +16,10 @@
 //     one texel, which the CFL limit gives at dyeScale 2 away from the fastest flow.  A
 //     sample outside the on-chip region is recomputed from global memory (the
 //     forward/backward values at that texel are re-derived), so the result does not
-//     depend on the halo being large enough.  Texture traffic drops from 7 texture passes to one read and one
-//     write.  The source, forward and backward windows hold binary16 texels, as those
-//     textures would (exact), and only r, g, b are carried: the corrected texel's
-//     alpha is 1 whatever the inputs.
+//     depend on the halo being large enough.  Texture traffic drops from 7 texture
+//     passes to one read and one write.  The source, forward and backward windows hold
+//     binary16 texels, as those textures would (exact), and only r, g, b are carried:
+//     the corrected texel's alpha is 1 whatever the inputs.
 #pragma once
 #include <cuda_fp16.h>
 #include "s2d_device.cuh"
