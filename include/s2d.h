@@ -122,6 +122,13 @@ int s2d_supported_grids(int* out, int capacity, int* count);
 int s2d_digit_reverse_table(int n, uint32_t* out /* n */);
 int s2d_wavenumber_table(int n, float* out /* n */);
 int s2d_dealias_mask_table(int n, uint8_t* out /* n*n */);
+/* Self-check of the fused dye kernel's tile geometry (no reference counterpart; host
+ * only, no GPU needed): for an n x n flow under an (n * dye_scale)^2 dye, every tile's
+ * traces shorter than one texel -- the tiles that skip the window bounds tests -- read
+ * only velocity cells inside the tile's velocity window and only dye texels inside the
+ * tile's source / forward / backward windows.  S2D_OK, or S2D_ERR_ARG naming the first
+ * tile and window that would be left. */
+int s2d_dye_fast_path_check(int n, int dye_scale);
 
 /* ---------------------------------------------------------------- lifecycle */
 /* Solver.create(device, {n, dyeScale}) (solver.js:71-140).  dye_scale is 1, 2 (the

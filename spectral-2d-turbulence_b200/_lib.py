@@ -95,6 +95,7 @@ PROTOTYPES = {
     "s2d_digit_reverse_table": (_i, [_i, C.POINTER(_u)]),
     "s2d_wavenumber_table": (_i, [_i, C.POINTER(_f)]),
     "s2d_dealias_mask_table": (_i, [_i, C.POINTER(C.c_uint8)]),
+    "s2d_dye_fast_path_check": (_i, [_i, _i]),
     "s2d_create": (_i, [_i, _i, _i, _i, C.POINTER(_vp)]),
     "s2d_destroy": (_i, [_vp]),
     "s2d_get_info": (_i, [_vp, C.POINTER(s2d_info)]),

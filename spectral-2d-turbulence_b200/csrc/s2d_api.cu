@@ -377,6 +377,60 @@ extern "C" int s2d_supported_grids(int* out, int capacity, int* count) {
   return S2D_OK;
 }
 
+// One axis of one tile of k_dye_fused: the tile starts at texel t0 and has T texels; the
+// backward / forward / source regions have W1 / W2 / W3 texels and the velocity window
+// vw cells, with the origins dye_cta_setup computes (src_lo: the source window's extra
+// texels below its halo).  A trace shorter than one texel from texel x has its bilinear
+// footprint's first texel at x - 1 or x, and its midpoint (half the displacement) reads
+// the velocity at a coordinate (x + 0.5 + d) n/m - 0.5 with |d| <= 1/2.
+static const char* dye_axis_check(int n, int m, int t0, int T, int W1, int W2, int W3, int src_lo, int vw) {
+  const long s_org = t0 - src_lo, f_org = t0 - 2 * kDyeLo, b_org = t0 - kDyeLo;
+  const long v_org = (long)floorf(((float)(t0 - 2 * kDyeLo - 1) + 0.5f) * (float)n / (float)m - 0.5f) - 1;
+  // slot of texel (or cell) t in a window at origin org holding w entries of a periodic
+  // axis of len: its lookup reads this slot and the next
+  auto fits = [](long t, long org, int w, int len) {
+    const long d = ((t - org) % len + len) % len;
+    return d + 1 < w;
+  };
+  auto footprints_in = [&](long x, long org, int w) { return fits(x - 1, org, w, m) && fits(x, org, w, m); };
+  auto velocity_in = [&](long x) {
+    for (int d = -1; d <= 1; ++d) {   // d / 2 texels: the midpoint extremes and the centre
+      const double g = ((double)x + 0.5 + 0.5 * d) * (double)n / (double)m - 0.5;
+      if (!fits((long)std::floor(g), v_org, vw, n)) return false;
+    }
+    return true;
+  };
+  for (long x = f_org; x < f_org + W2; ++x) {
+    if (!footprints_in(x, s_org, W3)) return "forward footprint outside the source window";
+    if (!velocity_in(x)) return "forward-region trace outside the velocity window";
+  }
+  for (long x = b_org; x < b_org + W1; ++x)
+    if (!footprints_in(x, f_org, W2)) return "backward footprint outside the forward window";
+  for (long x = t0; x < t0 + T; ++x) {
+    if (!footprints_in(x, s_org, W3)) return "corrected footprint outside the source window";
+    if (!footprints_in(x, b_org, W1)) return "corrected footprint outside the backward window";
+  }
+  return nullptr;
+}
+
+template <int TX> static int dye_fast_path_check_tx(int n, int m) {
+  using G = DyeGeom<TX>;
+  for (int t0 = 0; t0 < m; t0 += TX)
+    if (const char* why = dye_axis_check(n, m, t0, TX, G::W1X, G::W2X, G::W3X, 3 * kDyeLo + 1, G::vel_x(n, m)))
+      return fail(S2D_ERR_ARG, std::string("x tile at ") + std::to_string(t0) + ": " + why);
+  for (int t0 = 0; t0 < m; t0 += G::TY)
+    if (const char* why = dye_axis_check(n, m, t0, G::TY, G::W1Y, G::W2Y, G::W3Y, 3 * kDyeLo, G::vel_y(n, m)))
+      return fail(S2D_ERR_ARG, std::string("y tile at ") + std::to_string(t0) + ": " + why);
+  return S2D_OK;
+}
+
+extern "C" int s2d_dye_fast_path_check(int n, int dye_scale) {
+  if (n < S2D_MIN_N || n > S2D_MAX_N || (n & (n - 1)) != 0) return fail(S2D_ERR_UNSUPPORTED_N, "n");
+  if (dye_scale != 1 && dye_scale != 2 && dye_scale != 4) return fail(S2D_ERR_ARG, "dye_scale must be 1, 2 or 4");
+  const int m = n * dye_scale;
+  return dye_wide_tile(n, m) ? dye_fast_path_check_tx<64>(n, m) : dye_fast_path_check_tx<32>(n, m);
+}
+
 static int table_prelude(int n) {
   if (n < 2 || n > (1 << 16) || (n & (n - 1))) return fail(S2D_ERR_UNSUPPORTED_N, "size must be a power of two");
   int dev = 0;
