@@ -133,10 +133,20 @@ struct GraphEntry {
 static size_t diag_block_bytes(int nbins, int n) {
   return (sizeof(double) + sizeof(uint32_t)) * (size_t)(nbins + 2) + sizeof(float) * (size_t)n;
 }
-// the two dt slots follow the diagnostics block in its allocation, so that copyDiagnostics
-// reads both in one copy
+// Two diagnostics blocks, used in turn, around the two dt slots: [block 0][dt slots]
+// [block 1].  The diagnostics kernel accumulates into one block and clears the other for
+// the next call (no separate clear), and copyDiagnostics reads the block last filled and
+// the dt slots in one copy (block 0 + slots, or slots + block 1).
 static size_t diag_dt_offset(int nbins, int n) { return (diag_block_bytes(nbins, n) + 15) & ~size_t(15); }
-static size_t diag_alloc_bytes(int nbins, int n) { return diag_dt_offset(nbins, n) + 4 * sizeof(float); }
+static size_t diag_block_offset(int nbins, int n, int b) {
+  return b == 0 ? 0 : diag_dt_offset(nbins, n) + 4 * sizeof(float);
+}
+static size_t diag_alloc_bytes(int nbins, int n) { return diag_block_offset(nbins, n, 1) + diag_block_bytes(nbins, n); }
+// the range one copy reads for block b: the block and the dt slots
+static size_t diag_copy_offset(int nbins, int n, int b) { return b == 0 ? 0 : diag_dt_offset(nbins, n); }
+static size_t diag_copy_bytes(int nbins, int n, int b) {
+  return b == 0 ? diag_dt_offset(nbins, n) + 4 * sizeof(float) : 4 * sizeof(float) + diag_block_bytes(nbins, n);
+}
 
 constexpr int kUploadSlots = 8;
 constexpr size_t kUploadSlotBytes = 512;
@@ -158,12 +168,12 @@ struct s2d_solver {
   unsigned* ticket = nullptr;
   DevParams* dparams = nullptr;
   DevSplats* dsplats = nullptr;   // inside dparams' allocation, right after the parameters
-  // diagnostics block, one allocation (one clear, one readback copy): FP64 bins + totals
-  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n], then (16-byte
-  // aligned) the dt slots
-  double* diag = nullptr;
-  uint32_t* diag_fixed = nullptr;   // inside diag's allocation
-  float* zonal = nullptr;           // inside diag's allocation
+  // diagnostics blocks (see diag_block_offset), one allocation: each FP64 bins + totals
+  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n]; the dt slots
+  // (16-byte aligned) between the two
+  double* diag = nullptr;           // the allocation
+  int diag_next = 0;                // the block the next diagnostics launch fills (the other is clear)
+  int diag_last = 0;                // the block the last one filled
   double* seed_parts = nullptr;
   uint32_t* step_counter = nullptr;   // device copy of step_index for S2D_STEP_RELATCH
   int* err = nullptr;                 // device error word (bounded waits that gave up)
@@ -179,6 +189,7 @@ struct s2d_solver {
   float* h_zonal = nullptr;         // inside h_diag's allocation
   float* h_dt = nullptr;            // inside h_diag's allocation: both dt slots
   int h_dt_slot = 0;                // the slot current when the copy was enqueued
+  double* h_base = nullptr;         // the pinned allocation (h_diag etc. point at the copied block)
   cudaEvent_t diag_event = nullptr;
   // pinned upload ring for the per-step parameter and splat blocks: slot i is rewritten
   // only after the copy that last read it has run (upload_ev[i])
@@ -205,6 +216,19 @@ struct s2d_solver {
   double prof_ms[S2D_PROF_CLASSES] = {0};
   int prof_cnt[S2D_PROF_CLASSES] = {0};
 };
+
+// device block b of the diagnostics allocation: FP64 bins, u32 bins, zonal mean
+static double* diag_fp64(s2d_solver* s, int b) {
+  return reinterpret_cast<double*>(reinterpret_cast<char*>(s->diag) + diag_block_offset(s->nbins, s->n, b));
+}
+static uint32_t* diag_u32(s2d_solver* s, int b) { return reinterpret_cast<uint32_t*>(diag_fp64(s, b) + s->nbins + 2); }
+static float* diag_zonal(s2d_solver* s, int b) { return reinterpret_cast<float*>(diag_u32(s, b) + s->nbins + 2); }
+// point the host views at pinned block b (the one the last copy read)
+static void set_host_diag_block(s2d_solver* s, int b) {
+  s->h_diag = reinterpret_cast<double*>(reinterpret_cast<char*>(s->h_base) + diag_block_offset(s->nbins, s->n, b));
+  s->h_fixed = reinterpret_cast<uint32_t*>(s->h_diag + s->nbins + 2);
+  s->h_zonal = reinterpret_cast<float*>(s->h_fixed + s->nbins + 2);
+}
 
 // Row-stage variants of a solver: the registered FP32 shapes, plus (last index) the row
 // stage on the tensor cores for a tensor-core solver.
@@ -278,7 +302,7 @@ static void free_solver(s2d_solver* s) {
                       s->step_counter, s->err, s->tctab, s->row_nz, s->image, s->dye[0], s->dye[1], s->dye[2]};
   for (void* p : dev_ptrs)
     if (p) cudaFree(p);
-  void* host_ptrs[] = {s->h_diag, s->h_upload};
+  void* host_ptrs[] = {s->h_base, s->h_upload};
   for (void* p : host_ptrs)
     if (p) cudaFreeHost(p);
   if (s->diag_event) cudaEventDestroy(s->diag_event);
@@ -596,8 +620,7 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMalloc(&s->dparams, kConstBytes), "params");
   s->dsplats = reinterpret_cast<DevSplats*>(reinterpret_cast<char*>(s->dparams) + sizeof(DevParams));
   TRY(cudaMalloc(&s->diag, diag_alloc_bytes(s->nbins, n)), "diag");
-  s->diag_fixed = reinterpret_cast<uint32_t*>(s->diag + s->nbins + 2);
-  s->zonal = reinterpret_cast<float*>(s->diag_fixed + s->nbins + 2);
+  TRY(cudaMemsetAsync(s->diag, 0, diag_alloc_bytes(s->nbins, n), s->stream), "memset");   // both blocks clear
   s->dtbuf = reinterpret_cast<float*>(reinterpret_cast<char*>(s->diag) + diag_dt_offset(s->nbins, n));
   TRY(cudaMalloc(&s->seed_parts, sizeof(double) * seed_parts_count(n)), "seed partials");
   TRY(cudaMalloc(&s->step_counter, sizeof(uint32_t)), "step counter");
@@ -605,10 +628,10 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream), "memset");
   TRY(cudaMemsetAsync(s->step_counter, 0, sizeof(uint32_t), s->stream), "memset");
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
-  TRY(cudaMallocHost(&s->h_diag, diag_alloc_bytes(s->nbins, n)), "pinned diag");
-  s->h_fixed = reinterpret_cast<uint32_t*>(s->h_diag + s->nbins + 2);
-  s->h_zonal = reinterpret_cast<float*>(s->h_fixed + s->nbins + 2);
-  s->h_dt = reinterpret_cast<float*>(reinterpret_cast<char*>(s->h_diag) + diag_dt_offset(s->nbins, n));
+  TRY(cudaMallocHost(&s->h_base, diag_alloc_bytes(s->nbins, n)), "pinned diag");
+  std::memset(s->h_base, 0, diag_alloc_bytes(s->nbins, n));
+  s->h_dt = reinterpret_cast<float*>(reinterpret_cast<char*>(s->h_base) + diag_dt_offset(s->nbins, n));
+  set_host_diag_block(s, 0);
   TRY(cudaMallocHost(&s->h_upload, kUploadSlotBytes * kUploadSlots), "pinned upload ring");
   for (cudaEvent_t& ev : s->upload_ev) TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
   TRY(set_all_attrs(*ops), "kernel attributes");
@@ -1174,12 +1197,16 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
 extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
-  const int n = s->n, nb = s->nbins;
-  S2D_CUDA(cudaMemsetAsync(s->diag, 0, (sizeof(double) + sizeof(uint32_t)) * (nb + 2), s->stream));
+  const int n = s->n;
+  // fill the clear block, clear the other one for the next launch
+  const int b = s->diag_next;
   const unsigned blocks = (unsigned)(diag_tiles(n) + diag_zonal_ctas(n));
-  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->vel, s->diag, s->diag_fixed,
-                                                            s->zonal, n);
+  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->vel, diag_fp64(s, b),
+                                                            diag_u32(s, b), diag_zonal(s, b), n,
+                                                            diag_fp64(s, 1 - b), diag_u32(s, 1 - b));
   S2D_LAUNCHED();
+  s->diag_last = b;
+  s->diag_next = 1 - b;
   return S2D_OK;
 }
 
@@ -1187,9 +1214,12 @@ extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
   S2D_USE(s);
   if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
   DeviceGuard guard(s->dev);
-  // the diagnostics block and both dt slots in one copy; the slot current now is the one read
-  S2D_CUDA(cudaMemcpyAsync(s->h_diag, s->diag, diag_alloc_bytes(s->nbins, s->n), cudaMemcpyDeviceToHost,
-                           s->stream));
+  // the block last filled and both dt slots in one copy; the slot current now is the one read
+  const int b = s->diag_last;
+  const size_t off = diag_copy_offset(s->nbins, s->n, b);
+  S2D_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(s->h_base) + off, reinterpret_cast<char*>(s->diag) + off,
+                           diag_copy_bytes(s->nbins, s->n, b), cudaMemcpyDeviceToHost, s->stream));
+  set_host_diag_block(s, b);
   s->h_dt_slot = s->slot;
   S2D_CUDA(cudaEventRecord(s->diag_event, s->stream));
   s->read_state = 1;

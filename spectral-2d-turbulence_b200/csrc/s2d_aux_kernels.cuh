@@ -232,7 +232,10 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 // mod 2^32 in any order, so the result equals per-cell atomics bit for bit.  The first
 // CTAs take the zonal mean, one warp per two rows, issuing a lane's loads eight at a time
 // (with one load in flight per lane they took 6.2 us alone at 1024^2); with them the
-// 512 tile CTAs of 1024^2 still fit one wave at 4 CTAs per SM.
+// 512 tile CTAs of 1024^2 still fit one wave at 4 CTAs per SM.  The sums accumulate into
+// a block that is zero on entry; the first zonal CTA zeroes the caller's other block
+// (clear_out, clear_bins), so calls that alternate between two blocks need no clear of
+// their own.
 //
 // Per cell: the f32 bin round(sqrtf(k2)) is the reference's; the FP64 bin
 // floor(sqrt(k2) + 0.5) is the same integer corrected by one step with integer tests
@@ -257,9 +260,16 @@ __device__ __forceinline__ int diag_min_abs_wn(int i0, int len, int n) {
   return min(abs(a), abs(b));
 }
 __global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, const float2* __restrict__ vel,
-                                                  double* out, uint32_t* bins, float* zonal, int n) {
+                                                  double* out, uint32_t* bins, float* zonal, int n,
+                                                  double* clear_out, uint32_t* clear_bins) {
   const int zctas = diag_zonal_ctas(n);
   if ((int)blockIdx.x < zctas) {   // zonal mean of u, FP64 accumulation, one warp per two rows
+    if (blockIdx.x == 0) {   // zero the other block's sums for the next launch
+      for (int i = threadIdx.x; i < n / 2 + 3; i += blockDim.x) {
+        clear_out[i] = 0.0;
+        clear_bins[i] = 0u;
+      }
+    }
     const int lane = threadIdx.x & 31;
     const int nq = n / 2;   // float4 (two velocity cells) per row
 #pragma unroll 1
