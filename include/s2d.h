@@ -322,8 +322,9 @@ int s2d_profile_read(s2d_solver* s, double* ms /* S2D_PROF_CLASSES */, int* laun
 int s2d_cfl_dt_static(const void* vel, int n, float cfl, float dt_min, float dt_max, void* dt_out, void* stream);
 
 /* ---------------------------------------------------------------- ensemble */
-/* Many independent instances of uneven sizes stepped together (no reference
- * counterpart beyond running many Solvers; BASELINE batching form). */
+/* Many independent instances of uneven sizes stepped together, each with its own
+ * viscosity, beta, drag and forcing (no reference counterpart beyond running
+ * many Solvers). */
 typedef struct s2d_instance_desc {
   int32_t n;              /* 64..1024, power of two */
   float beta, drag, nu_h; /* nu_h directly (not the rate) */
