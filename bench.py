@@ -464,10 +464,9 @@ def run_ours(args):
     e2e_value = world * e2e_steps / e2e_s
     nb = N // 2 + 1
     h2d = 64 + 16 + 8 * 48
-    # one copy per step: a diagnostics block (FP64 bins + u32 bins (+ totals), the zonal
-    # mean) and both dt slots; the two blocks alternate, the first padded to 16 bytes
-    block = (nb + 2) * 8 + (nb + 2) * 4 + N * 4
-    d2h = (block + 15) // 16 * 16 // 2 + block // 2 + 4 * 4
+    # two copies per step on the diagnostics stream: a diagnostics block (FP64 bins + u32
+    # bins (+ totals), the zonal mean) and the current [dt, speed] slot
+    d2h = (nb + 2) * 8 + (nb + 2) * 4 + N * 4 + 2 * 4
     finite = d is not None and all(map(lambda v: v == v, [d["energy"], d["enstrophy"], d["dt"]]))
     solver.destroy()
 

@@ -130,23 +130,18 @@ struct GraphEntry {
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> events;
 };
 
+// One diagnostics block: FP64 bins + energy + enstrophy [nbins + 2], u32 fixed-point bins
+// + totals [nbins + 2], zonal mean [n].
 static size_t diag_block_bytes(int nbins, int n) {
   return (sizeof(double) + sizeof(uint32_t)) * (size_t)(nbins + 2) + sizeof(float) * (size_t)n;
 }
-// Two diagnostics blocks, used in turn, around the two dt slots: [block 0][dt slots]
-// [block 1].  The diagnostics kernel accumulates into one block and clears the other for
-// the next call (no separate clear), and copyDiagnostics reads the block last filled and
-// the dt slots in one copy (block 0 + slots, or slots + block 1).
-static size_t diag_dt_offset(int nbins, int n) { return (diag_block_bytes(nbins, n) + 15) & ~size_t(15); }
-static size_t diag_block_offset(int nbins, int n, int b) {
-  return b == 0 ? 0 : diag_dt_offset(nbins, n) + 4 * sizeof(float);
-}
-static size_t diag_alloc_bytes(int nbins, int n) { return diag_block_offset(nbins, n, 1) + diag_block_bytes(nbins, n); }
-// the range one copy reads for block b: the block and the dt slots
-static size_t diag_copy_offset(int nbins, int n, int b) { return b == 0 ? 0 : diag_dt_offset(nbins, n); }
-static size_t diag_copy_bytes(int nbins, int n, int b) {
-  return b == 0 ? diag_dt_offset(nbins, n) + 4 * sizeof(float) : 4 * sizeof(float) + diag_block_bytes(nbins, n);
-}
+// Two blocks, used in turn, then the two dt slots: [block 0][block 1][dt slots], each part
+// 16-byte aligned.  Each diagnostics call fills one block and clears the sums of the other
+// for the next call (no separate clear).
+static size_t diag_block_stride(int nbins, int n) { return (diag_block_bytes(nbins, n) + 15) & ~size_t(15); }
+static size_t diag_block_offset(int nbins, int n, int b) { return (size_t)b * diag_block_stride(nbins, n); }
+static size_t diag_dt_offset(int nbins, int n) { return 2 * diag_block_stride(nbins, n); }
+static size_t diag_alloc_bytes(int nbins, int n) { return diag_dt_offset(nbins, n) + 4 * sizeof(float); }
 
 constexpr int kUploadSlots = 8;
 constexpr size_t kUploadSlotBytes = 512;
@@ -158,19 +153,28 @@ static_assert(sizeof(DevParams) % 16 == 0, "splat block alignment");
 
 struct s2d_solver {
   int dev = 0, n = 0, m = 0, nbins = 0, dye_scale = 1, fft_precision = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;        // every launch except the diagnostics below (high priority)
+  // Diagnostics stream (low priority): the k-space spectra of encodeDiagnostics and the
+  // readback copies run there, behind the work the main stream had enqueued, and alongside
+  // the next step.  The spectra read state[phase] of the step before them, which the next
+  // fused step reads but does not write; every other call that enqueues device work first
+  // orders the main stream after them (diag_order).
+  cudaStream_t diag_stream = nullptr;
+  cudaEvent_t diag_ready = nullptr;     // main-stream point the diagnostics stream waits for
+  cudaEvent_t diag_done = nullptr;      // the last spectra launch has finished
+  bool diag_outstanding = false;        // diag_done not yet waited for by the main stream
+  int diag_age = 0;                     // steps enqueued since the outstanding spectra launch
+  int in_step = 0;                      // inside a step call (its inner entry points do not order)
   const NOps* ops = nullptr;
   float2* state[3] = {nullptr, nullptr, nullptr};
   float2 *packA = nullptr, *packB = nullptr, *physZ = nullptr, *rhs = nullptr, *force = nullptr,
          *vel = nullptr, *tw = nullptr;
-  float* dtbuf = nullptr;      // 2 slots x [dt, speed], inside diag's allocation
+  float* dtbuf = nullptr;      // 2 slots x [dt, speed], at the end of diag's allocation
   float* partials = nullptr;
   unsigned* ticket = nullptr;
   DevParams* dparams = nullptr;
   DevSplats* dsplats = nullptr;   // inside dparams' allocation, right after the parameters
-  // diagnostics blocks (see diag_block_offset), one allocation: each FP64 bins + totals
-  // [nbins + 2], u32 fixed-point bins + totals [nbins + 2], zonal mean [n]; the dt slots
-  // (16-byte aligned) between the two
+  // the two diagnostics blocks and the dt slots in one allocation (diag_block_offset)
   double* diag = nullptr;           // the allocation
   int diag_next = 0;                // the block the next diagnostics launch fills (the other is clear)
   int diag_last = 0;                // the block the last one filled
@@ -187,8 +191,7 @@ struct s2d_solver {
   double* h_diag = nullptr;
   uint32_t* h_fixed = nullptr;      // inside h_diag's allocation
   float* h_zonal = nullptr;         // inside h_diag's allocation
-  float* h_dt = nullptr;            // inside h_diag's allocation: both dt slots
-  int h_dt_slot = 0;                // the slot current when the copy was enqueued
+  float* h_dt = nullptr;            // inside h_base: [dt, speed] of the slot current at the copy
   double* h_base = nullptr;         // the pinned allocation (h_diag etc. point at the copied block)
   cudaEvent_t diag_event = nullptr;
   // pinned upload ring for the per-step parameter and splat blocks: slot i is rewritten
@@ -283,6 +286,7 @@ struct ProfScope {
 static int seed_parts_count(int n) { return (n * n + 255) / 256; }
 
 static void free_solver(s2d_solver* s) {
+  if (s->diag_stream) cudaStreamSynchronize(s->diag_stream);   // its copies read device memory
   for (auto& kv : s->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -305,9 +309,11 @@ static void free_solver(s2d_solver* s) {
   void* host_ptrs[] = {s->h_base, s->h_upload};
   for (void* p : host_ptrs)
     if (p) cudaFreeHost(p);
-  if (s->diag_event) cudaEventDestroy(s->diag_event);
+  for (cudaEvent_t ev : {s->diag_event, s->diag_ready, s->diag_done})
+    if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : s->upload_ev)
     if (ev) cudaEventDestroy(ev);
+  if (s->diag_stream) cudaStreamDestroy(s->diag_stream);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -347,11 +353,34 @@ static int flush_uploads(s2d_solver* s) {
     if (!(s)) return fail(S2D_ERR_ARG, "null solver handle");              \
     if ((s)->disposed) return fail(S2D_ERR_DESTROYED, "solver destroyed"); \
   } while (0)
-#define S2D_USE(s)                                   \
+// the main stream waits for the outstanding spectra launch (see s2d_solver::diag_stream)
+static int diag_order(s2d_solver* s) {
+  if (!s->diag_outstanding) return S2D_OK;
+  s->diag_outstanding = false;
+  const cudaError_t e = cudaStreamWaitEvent(s->stream, s->diag_done, 0);
+  return e == cudaSuccess ? S2D_OK : fail(S2D_ERR_CUDA, std::string("diagnostics order: ") + cudaGetErrorString(e));
+}
+// Every entry point that enqueues device work (or reads the device) flushes the host
+// blocks and orders the main stream after the outstanding spectra; the step entry points
+// order only where a step may write what the spectra read (diag_order_step), and the
+// readback calls, which use the diagnostics stream, do not order.
+#define S2D_USE_NOORDER(s)                           \
   do {                                               \
     S2D_USE_HOST(s);                                 \
     if (int rc_ = flush_uploads(s)) return rc_;      \
   } while (0)
+#define S2D_USE(s)                                                    \
+  do {                                                                \
+    S2D_USE_NOORDER(s);                                               \
+    if (!(s)->in_step)                                                \
+      if (int rc_ = diag_order(s)) return rc_;                        \
+  } while (0)
+// marks the body of a step call: its inner entry points leave the ordering to it
+struct InStep {
+  s2d_solver* s;
+  explicit InStep(s2d_solver* s_) : s(s_) { ++s->in_step; }
+  ~InStep() { --s->in_step; }
+};
 
 // ------------------------------------------------------------------ library entry points
 extern "C" int s2d_version(void) { return 10000; }
@@ -602,8 +631,14 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
 #define TRY(call, what)            \
   if ((e = (call)) != cudaSuccess) \
     return bail(e, what);
-  TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  // the step work ahead of the diagnostics spectra when both have CTAs waiting for an SM
+  int prio_least = 0, prio_greatest = 0;
+  TRY(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest), "stream priorities");
+  TRY(cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, prio_greatest), "stream");
+  TRY(cudaStreamCreateWithPriority(&s->diag_stream, cudaStreamNonBlocking, prio_least), "diagnostics stream");
   TRY(cudaEventCreateWithFlags(&s->diag_event, cudaEventDisableTiming), "event");
+  TRY(cudaEventCreateWithFlags(&s->diag_ready, cudaEventDisableTiming), "event");
+  TRY(cudaEventCreateWithFlags(&s->diag_done, cudaEventDisableTiming), "event");
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->state[i], cbytes), "state");
   TRY(cudaMalloc(&s->packA, cbytes), "packA");
   TRY(cudaMalloc(&s->packB, cbytes), "packB");
@@ -630,7 +665,7 @@ extern "C" int s2d_create(int n, int dye_scale, int fft_precision, int device, s
   for (int i = 0; i < 3; ++i) TRY(cudaMalloc(&s->dye[i], dbytes), "dye");
   TRY(cudaMallocHost(&s->h_base, diag_alloc_bytes(s->nbins, n)), "pinned diag");
   std::memset(s->h_base, 0, diag_alloc_bytes(s->nbins, n));
-  s->h_dt = reinterpret_cast<float*>(reinterpret_cast<char*>(s->h_base) + diag_dt_offset(s->nbins, n));
+  s->h_dt = reinterpret_cast<float*>(reinterpret_cast<char*>(s->h_base) + diag_dt_offset(s->nbins, n));   // [dt, speed]
   set_host_diag_block(s, 0);
   TRY(cudaMallocHost(&s->h_upload, kUploadSlotBytes * kUploadSlots), "pinned upload ring");
   for (cudaEvent_t& ev : s->upload_ev) TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
@@ -691,6 +726,7 @@ extern "C" int s2d_destroy(s2d_solver* s) {
   if (!s) return fail(S2D_ERR_ARG, "null solver handle");
   DeviceGuard guard(s->dev);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->diag_stream) cudaStreamSynchronize(s->diag_stream);
   s->disposed = true;
   free_solver(s);
   delete s;
@@ -776,6 +812,7 @@ extern "C" int s2d_synchronize(s2d_solver* s) {
   S2D_USE(s);
   DeviceGuard guard(s->dev);
   S2D_CUDA(cudaStreamSynchronize(s->stream));
+  S2D_CUDA(cudaStreamSynchronize(s->diag_stream));
   return check_device_error(s);
 }
 
@@ -1097,10 +1134,22 @@ static int enqueue_relatch(s2d_solver* s) {
   return S2D_OK;
 }
 
+// A fused step reads state[phase] (as w0) and writes the other two ring buffers, the
+// packs, the velocity, the dye and the other dt slot, so one such step may run alongside
+// the outstanding spectra (which read state[phase] of the step before it); the step after
+// it writes that buffer, and the unfused tensor-core steps use the ring differently.
+static int diag_order_step(s2d_solver* s, int substeps) {
+  if (!s->diag_outstanding) return S2D_OK;
+  if (s->diag_age == 0 && substeps <= 1 && !tc_unfused(s)) return S2D_OK;
+  return diag_order(s);
+}
+
 extern "C" int s2d_step(s2d_solver* s, int substeps, unsigned flags) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   if (substeps < 0) return fail(S2D_ERR_ARG, "substeps < 0");
   DeviceGuard guard(s->dev);
+  if (int rc = diag_order_step(s, substeps)) return rc;
+  InStep in_step(s);
   if (!s->primed)
     if (int rc = s2d_encode_prime(s)) return rc;
   if (flags & S2D_STEP_RELATCH)
@@ -1113,14 +1162,17 @@ extern "C" int s2d_step(s2d_solver* s, int substeps, unsigned flags) {
       if (int rc = s2d_encode_dye(s)) return rc;
     if (flags & S2D_STEP_REDUCE)
       if (int rc = s2d_encode_reduce(s)) return rc;
+    ++s->diag_age;
   }
   return S2D_OK;
 }
 
 extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   if (substeps < 0) return fail(S2D_ERR_ARG, "substeps < 0");
   DeviceGuard guard(s->dev);
+  if (int rc = diag_order_step(s, substeps)) return rc;
+  InStep in_step(s);
   if (!s->primed)
     if (int rc = s2d_encode_prime(s)) return rc;
   if (!s->packs_valid && !tc_unfused(s))
@@ -1189,52 +1241,64 @@ extern "C" int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags) {
       s->slot ^= 1;
       s->reduced_valid = false;
     }
+    ++s->diag_age;
   }
   return S2D_OK;
 }
 
 // ------------------------------------------------------------------ diagnostics
 extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
-  S2D_USE(s);
+  S2D_USE(s);   // the previous spectra (and the copies before them) are done before this block is written
   DeviceGuard guard(s->dev);
   const int n = s->n;
-  // fill the clear block, clear the other one for the next launch
+  // fill the clear block; the spectra clear the other one for the next call
   const int b = s->diag_next;
-  const unsigned blocks = (unsigned)(diag_tiles(n) + diag_zonal_ctas(n));
-  k_diag_all<<<blocks, 256, diag_all_smem(n), s->stream>>>(s->state[s->phase], s->vel, diag_fp64(s, b),
-                                                            diag_u32(s, b), diag_zonal(s, b), n,
-                                                            diag_fp64(s, 1 - b), diag_u32(s, 1 - b));
+  // the zonal mean reads the velocity, which the next step rewrites: on the main stream
+  k_diag_zonal<<<diag_zonal_ctas(n), 256, 0, s->stream>>>(s->vel, diag_zonal(s, b), n);
   S2D_LAUNCHED();
+  // the spectra of state[phase] on the diagnostics stream, alongside the next step
+  S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
+  S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
+  k_diag_tiles<<<diag_tiles(n), 256, diag_all_smem(n), s->diag_stream>>>(
+      s->state[s->phase], diag_fp64(s, b), diag_u32(s, b), n, diag_fp64(s, 1 - b), diag_u32(s, 1 - b));
+  S2D_LAUNCHED();
+  S2D_CUDA(cudaEventRecord(s->diag_done, s->diag_stream));
+  s->diag_outstanding = true;
+  s->diag_age = 0;
   s->diag_last = b;
   s->diag_next = 1 - b;
   return S2D_OK;
 }
 
 extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
   DeviceGuard guard(s->dev);
-  // the block last filled and both dt slots in one copy; the slot current now is the one read
+  // on the diagnostics stream, behind the spectra and the main stream's work so far: the
+  // block last filled, and the [dt, speed] slot current now
+  S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
+  S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
   const int b = s->diag_last;
-  const size_t off = diag_copy_offset(s->nbins, s->n, b);
+  const size_t off = diag_block_offset(s->nbins, s->n, b);
   S2D_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(s->h_base) + off, reinterpret_cast<char*>(s->diag) + off,
-                           diag_copy_bytes(s->nbins, s->n, b), cudaMemcpyDeviceToHost, s->stream));
+                           diag_block_bytes(s->nbins, s->n), cudaMemcpyDeviceToHost, s->diag_stream));
+  S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), 2 * sizeof(float), cudaMemcpyDeviceToHost,
+                           s->diag_stream));
   set_host_diag_block(s, b);
-  s->h_dt_slot = s->slot;
-  S2D_CUDA(cudaEventRecord(s->diag_event, s->stream));
+  S2D_CUDA(cudaEventRecord(s->diag_event, s->diag_stream));
   s->read_state = 1;
   return S2D_OK;
 }
 
 extern "C" int s2d_poll_diagnostics(s2d_solver* s) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   if (s->read_state != 1) return 0;
   return cudaEventQuery(s->diag_event) == cudaSuccess ? 1 : 0;
 }
 
 extern "C" int s2d_read_diagnostics(s2d_solver* s, double* spectrum, float* zonal, double* energy,
                                     double* enstrophy, float* dt, float* max_speed) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   if (s->read_state != 1) return S2D_NO_DATA;
   DeviceGuard guard(s->dev);
   cudaError_t e = cudaEventSynchronize(s->diag_event);
@@ -1245,13 +1309,13 @@ extern "C" int s2d_read_diagnostics(s2d_solver* s, double* spectrum, float* zona
   if (zonal) std::memcpy(zonal, s->h_zonal, sizeof(float) * s->n);
   if (energy) *energy = s->h_diag[nb];
   if (enstrophy) *enstrophy = s->h_diag[nb + 1];
-  if (dt) *dt = s->h_dt[2 * s->h_dt_slot];
-  if (max_speed) *max_speed = s->h_dt[2 * s->h_dt_slot + 1];
+  if (dt) *dt = s->h_dt[0];
+  if (max_speed) *max_speed = s->h_dt[1];
   return S2D_OK;
 }
 
 extern "C" int s2d_read_diagnostics_fixed(s2d_solver* s, float* spectrum, float* energy, float* enstrophy) {
-  S2D_USE(s);
+  S2D_USE_NOORDER(s);
   DeviceGuard guard(s->dev);
   S2D_CUDA(cudaEventSynchronize(s->diag_event));
   const int nb = s->nbins;

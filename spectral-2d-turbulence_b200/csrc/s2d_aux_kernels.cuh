@@ -213,10 +213,35 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 }
 
 // ------------------------------------------------------------------ diagnostics
+// The zonal mean of u (spectrum.wgsl:41-68), FP64 sums: one warp per row, a lane's loads
+// issued eight at a time (with one load in flight per lane the zonal mean took 6.2 us
+// alone at 1024^2).  Lane order i = lane + 32 j within a row, then the warp sum.
+__host__ __device__ constexpr int diag_zonal_ctas(int n) { return (n + 7) / 8; }
+__global__ void __launch_bounds__(256) k_diag_zonal(const float2* __restrict__ vel, float* zonal, int n) {
+  const int lane = threadIdx.x & 31;
+  const int row = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
+  if (row >= n) return;
+  const int nq = n / 2;   // float4 (two velocity cells) per row
+  const float4* r4 = reinterpret_cast<const float4*>(vel + (size_t)row * n);
+  double acc = 0.0;
+  for (int base = lane; base < nq; base += 32 * 8) {
+    float4 t[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) t[j] = base + 32 * j < nq ? r4[base + 32 * j] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (base + 32 * j < nq) {
+        acc += (double)t[j].x;
+        acc += (double)t[j].z;
+      }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) zonal[row] = (float)(acc / n);
+}
+
 // Both spectra in one pass over the state: the FP64 radial spectrum, energy and
 // enstrophy (spectral2d.py:92-104) and the reference's u32 fixed-point bins,
-// truncating, in the dealias band (spectrum.wgsl:19-39); the zonal mean of u
-// (spectrum.wgsl:41-68) in the same launch.
+// truncating, in the dealias band (spectrum.wgsl:19-39).
 //
 // A CTA takes a k-space tile of TW x TH cells (TW = min(64, n), TW * TH = 2048).  The
 // cells of a tile span fewer than kDiagSpan radial bins (its diagonal is < 72), so each
@@ -229,13 +254,10 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 // memory once per CTA (18.5 -> 14.4 us at 1024^2 against one shared FP64 array whose
 // words the 8 threads of a tile row hit together).  The u32 fixed-point bins use one
 // shared array: the u32 sums wrap
-// mod 2^32 in any order, so the result equals per-cell atomics bit for bit.  The first
-// CTAs take the zonal mean, one warp per two rows, issuing a lane's loads eight at a time
-// (with one load in flight per lane they took 6.2 us alone at 1024^2); with them the
-// 512 tile CTAs of 1024^2 still fit one wave at 4 CTAs per SM.  The sums accumulate into
-// a block that is zero on entry; the first zonal CTA zeroes the caller's other block
-// (clear_out, clear_bins), so calls that alternate between two blocks need no clear of
-// their own.
+// mod 2^32 in any order, so the result equals per-cell atomics bit for bit.  The sums
+// accumulate into a block that is zero on entry; the first CTA zeroes the caller's other
+// block (clear_out, clear_bins), so calls that alternate between two blocks need no clear
+// of their own.
 //
 // Per cell: the f32 bin round(sqrtf(k2)) is the reference's; the FP64 bin
 // floor(sqrt(k2) + 0.5) is the same integer corrected by one step with integer tests
@@ -247,7 +269,6 @@ constexpr int kDiagStride = kDiagSpan + 1;   // odd double stride: the 32 lanes'
 __host__ __device__ constexpr int diag_tile_w(int n) { return n < 64 ? n : 64; }
 __host__ __device__ constexpr int diag_tile_h(int n) { return 2048 / diag_tile_w(n) < n ? 2048 / diag_tile_w(n) : n; }
 __host__ __device__ constexpr int diag_tiles(int n) { return (n / diag_tile_w(n)) * (n / diag_tile_h(n)); }
-__host__ __device__ constexpr int diag_zonal_ctas(int n) { return (n + 15) / 16; }
 __host__ __device__ constexpr size_t diag_all_smem(int n) {
   return sizeof(double) * (32 * kDiagStride + 2) + sizeof(uint32_t) * (size_t)(n / 2 + 3);
 }
@@ -259,43 +280,15 @@ __device__ __forceinline__ int diag_min_abs_wn(int i0, int len, int n) {
   if (a > b) return 0;   // the range crosses n/2 (both signs present)
   return min(abs(a), abs(b));
 }
-__global__ void __launch_bounds__(256) k_diag_all(const float2* __restrict__ w, const float2* __restrict__ vel,
-                                                  double* out, uint32_t* bins, float* zonal, int n,
-                                                  double* clear_out, uint32_t* clear_bins) {
-  const int zctas = diag_zonal_ctas(n);
-  if ((int)blockIdx.x < zctas) {   // zonal mean of u, FP64 accumulation, one warp per two rows
-    if (blockIdx.x == 0) {   // zero the other block's sums for the next launch
-      for (int i = threadIdx.x; i < n / 2 + 3; i += blockDim.x) {
-        clear_out[i] = 0.0;
-        clear_bins[i] = 0u;
-      }
+__global__ void __launch_bounds__(256) k_diag_tiles(const float2* __restrict__ w, double* out, uint32_t* bins,
+                                                    int n, double* clear_out, uint32_t* clear_bins) {
+  if (blockIdx.x == 0) {   // zero the other block's sums for the next launch
+    for (int i = threadIdx.x; i < n / 2 + 3; i += blockDim.x) {
+      clear_out[i] = 0.0;
+      clear_bins[i] = 0u;
     }
-    const int lane = threadIdx.x & 31;
-    const int nq = n / 2;   // float4 (two velocity cells) per row
-#pragma unroll 1
-    for (int r = 0; r < 2; ++r) {
-      const int row = (int)blockIdx.x * 16 + (int)(threadIdx.x >> 5) * 2 + r;
-      if (row >= n) return;
-      const float4* r4 = reinterpret_cast<const float4*>(vel + (size_t)row * n);
-      double acc = 0.0;
-      // lane order i = lane + 32 j, as one load at a time would sum them
-      for (int base = lane; base < nq; base += 32 * 8) {
-        float4 t[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) t[j] = base + 32 * j < nq ? r4[base + 32 * j] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (base + 32 * j < nq) {
-            acc += (double)t[j].x;
-            acc += (double)t[j].z;
-          }
-      }
-      acc = warp_sum(acc);
-      if (lane == 0) zonal[row] = (float)(acc / n);
-    }
-    return;
   }
-  const int tile = (int)blockIdx.x - zctas;
+  const int tile = (int)blockIdx.x;
   extern __shared__ double win[];                      // [32 lanes][kDiagStride], then 2 totals
   double* const tot = win + 32 * kDiagStride;
   uint32_t* const fhist = reinterpret_cast<uint32_t*>(tot + 2);

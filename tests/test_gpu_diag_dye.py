@@ -22,6 +22,102 @@ def test_read_before_copy_is_null(pkg):
         s.destroy()
 
 
+def _same_diagnostics(a, b, what):
+    """Diagnostics of one state: the zonal mean bit for bit, the FP64 sums (added across
+    CTAs in any order) to their rounding."""
+    assert np.array_equal(a["zonal"], b["zonal"]), what
+    assert np.allclose(a["spectrum"], b["spectrum"], rtol=1e-13, atol=1e-300), what
+    for key in ("energy", "enstrophy"):
+        assert abs(a[key] - b[key]) <= 1e-13 * abs(b[key]), (what, key)
+
+
+def _diag_after_steps(pkg, n, steps, graph, between):
+    """Diagnostics of the state after `steps` steps, with `between(s)` run between
+    encodeDiagnostics and copyDiagnostics; returns the read result and the dt slots read
+    after it."""
+    s = pkg.Solver.create(n=n, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
+        s.seedPhysical(random_field(n, k0=n / 10, seed=11, amplitude=5.0))
+        for _ in range(steps):
+            s.step(1, dye=True, reduce=True, graph=graph)
+        s.encodeDiagnostics()
+        between(s)
+        s.copyDiagnostics()
+        d = s.readDiagnostics()
+        return d, s.getBuffer("dt")[:2].copy()
+    finally:
+        s.destroy()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_diagnostics_run_alongside_the_next_steps(pkg, graph):
+    """The spectra run on a second stream alongside the next step, and the calls after them
+    are ordered so that the result is the state at encodeDiagnostics: steps (one, then a
+    second that rewrites the state buffer the spectra read), a reseed, a second encode and
+    multi-substep calls leave it unchanged (the zonal mean bit for bit, the FP64 sums to
+    their rounding: CTAs add them in any order; a spectrum of a later state would differ in
+    the third digit); dt is the slot current at the copy (solver.js:560-568)."""
+    n = 256
+    base, _ = _diag_after_steps(pkg, n, 3, graph, lambda s: None)
+    cases = {
+        "one step": lambda s: s.step(1, dye=True, reduce=True, graph=graph),
+        "three steps": lambda s: [s.step(1, dye=True, reduce=True, graph=graph) for _ in range(3)],
+        "substeps": lambda s: s.step(4, dye=True, reduce=True, graph=graph),
+        "reseed": lambda s: s.seed(k0=9, amplitude=3, seed=5),
+    }
+    for name, between in cases.items():
+        d, dt_now = _diag_after_steps(pkg, n, 3, graph, between)
+        _same_diagnostics(d, base, name)
+        assert d["dt"] == dt_now[0] and d["maxSpeed"] == dt_now[1], name
+
+    # a second encode before the copy: the copy reads the later block, equal to the
+    # diagnostics of the same state encoded once
+    def twice(s):
+        s.step(1, dye=True, reduce=True, graph=graph)
+        s.encodeDiagnostics()
+    d2, _ = _diag_after_steps(pkg, n, 3, graph, twice)
+    once, _ = _diag_after_steps(pkg, n, 4, graph, lambda s: None)
+    _same_diagnostics(d2, once, "second encode")
+
+
+def test_pipelined_readback_matches_synchronous(pkg):
+    """The frame-loop order of the end-to-end benchmark (step k, encode k, read k-1,
+    copy k) gives, for every step, the diagnostics a synchronous encode-copy-read of the
+    same state gives."""
+    n, steps = 128, 6
+    sync = []
+    s = pkg.Solver.create(n=n, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
+        s.seedPhysical(random_field(n, k0=12, seed=4, amplitude=5.0))
+        for _ in range(steps):
+            s.step(1, dye=True, reduce=True, graph=True)
+            s.encodeDiagnostics(); s.copyDiagnostics()
+            sync.append(s.readDiagnostics())
+    finally:
+        s.destroy()
+    piped = []
+    s = pkg.Solver.create(n=n, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
+        s.seedPhysical(random_field(n, k0=12, seed=4, amplitude=5.0))
+        for _ in range(steps):
+            s.step(1, dye=True, reduce=True, graph=True)
+            s.encodeDiagnostics()
+            d = s.readDiagnostics()
+            if d is not None:
+                piped.append(d)
+            s.copyDiagnostics()
+        piped.append(s.readDiagnostics())
+    finally:
+        s.destroy()
+    assert len(piped) == steps
+    for k, (a, b) in enumerate(zip(sync, piped)):
+        _same_diagnostics(a, b, k)
+        assert a["dt"] == b["dt"] and a["maxSpeed"] == b["maxSpeed"], k
+
+
 @pytest.mark.parametrize("n", [32, 64, 512, 2048])
 def test_fp64_diagnostics(pkg, n):
     """Every k-space tile geometry of the diagnostics kernel: a tile spanning the whole
