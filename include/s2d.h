@@ -140,8 +140,11 @@ int s2d_get_info(s2d_solver* s, s2d_info* out);
 /* solver.phase / dyeParity / simTime assignments made by tests/index.html:162,185-186 */
 int s2d_set_phase(s2d_solver* s, int phase, int dye_parity);
 int s2d_set_sim_time(s2d_solver* s, double t);
-/* CUDA stream the solver enqueues on (cudaStream_t as void*). */
+/* CUDA stream the solver enqueues on (cudaStream_t as void*), created at the highest
+ * stream priority.  The diagnostics spectra and readback copies run on a second,
+ * lowest-priority stream of the solver (see s2d_encode_diagnostics). */
 int s2d_get_stream(s2d_solver* s, void** stream);
+/* Waits for both streams and reports a bounded device-side wait that gave up. */
 int s2d_synchronize(s2d_solver* s);
 /* Failure-detection check (no reference counterpart; the reference's WebGPU queue has no
  * device-side waits).  Every device-side wait of the library (bulk-copy and MMA
@@ -248,8 +251,17 @@ int s2d_step(s2d_solver* s, int substeps, unsigned flags);
 int s2d_step_graph(s2d_solver* s, int substeps, unsigned flags);
 
 /* ---------------------------------------------------------------- diagnostics */
-int s2d_encode_diagnostics(s2d_solver* s);                               /* solver.js:547-558 */
-int s2d_copy_diagnostics(s2d_solver* s);                                 /* solver.js:560-568 */
+/* Diagnostics of the current state (solver.js:547-558): the zonal mean on the solver's
+ * stream; the FP64 and fixed-point spectra on the solver's diagnostics stream, behind
+ * the work enqueued so far, so that they run alongside the next step.  The library
+ * orders its later calls after them where they would change what the spectra read (a
+ * step call waits for them unless it is one fused step right after them), so the
+ * results are those of the state at this call. */
+int s2d_encode_diagnostics(s2d_solver* s);
+/* solver.js:560-568: on the diagnostics stream, behind the spectra and the work enqueued
+ * so far, copies the block the last s2d_encode_diagnostics filled and the [dt, speed]
+ * slot current now. */
+int s2d_copy_diagnostics(s2d_solver* s);
 /* 1 when the copied diagnostics have landed in host memory, 0 otherwise. */
 int s2d_poll_diagnostics(s2d_solver* s);
 /* readDiagnostics() (solver.js:570-608): waits for the copy; S2D_NO_DATA when
