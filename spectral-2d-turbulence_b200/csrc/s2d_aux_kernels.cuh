@@ -214,22 +214,25 @@ __global__ void k_scale_spectrum(float2* data, const double* partial, int nparts
 
 // ------------------------------------------------------------------ diagnostics
 // The zonal mean of u (spectrum.wgsl:41-68), FP64 sums: one warp per row, a lane's loads
-// issued eight at a time (with one load in flight per lane the zonal mean took 6.2 us
-// alone at 1024^2).  Lane order i = lane + 32 j within a row, then the warp sum.
+// issued sixteen at a time (a whole 1024-cell row in one round trip; with one load in
+// flight per lane the zonal mean took 6.2 us alone at 1024^2).  Lane order i = lane + 32 j
+// within a row, then the warp sum.
 __host__ __device__ constexpr int diag_zonal_ctas(int n) { return (n + 7) / 8; }
 __global__ void __launch_bounds__(256) k_diag_zonal(const float2* __restrict__ vel, float* zonal, int n) {
+  constexpr int kBatch = 16;
   const int lane = threadIdx.x & 31;
   const int row = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
   if (row >= n) return;
   const int nq = n / 2;   // float4 (two velocity cells) per row
   const float4* r4 = reinterpret_cast<const float4*>(vel + (size_t)row * n);
   double acc = 0.0;
-  for (int base = lane; base < nq; base += 32 * 8) {
-    float4 t[8];
+  for (int base = lane; base < nq; base += 32 * kBatch) {
+    float4 t[kBatch];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) t[j] = base + 32 * j < nq ? r4[base + 32 * j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 0; j < kBatch; ++j)
+      t[j] = base + 32 * j < nq ? __ldcs(r4 + base + 32 * j) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < kBatch; ++j)
       if (base + 32 * j < nq) {
         acc += (double)t[j].x;
         acc += (double)t[j].z;
@@ -294,7 +297,9 @@ __global__ void __launch_bounds__(256) k_diag_tiles(const float2* __restrict__ w
   uint32_t* const fhist = reinterpret_cast<uint32_t*>(tot + 2);
   const int nb = n / 2 + 1;
   const int lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < 32 * kDiagStride + 2; i += blockDim.x) win[i] = 0.0;
+  static_assert((32 * kDiagStride + 2) % 2 == 0, "windows and totals cleared in 16-byte stores");
+  for (int i = threadIdx.x; i < (32 * kDiagStride + 2) / 2; i += blockDim.x)
+    reinterpret_cast<double2*>(win)[i] = make_double2(0.0, 0.0);
   for (int i = threadIdx.x; i < nb + 2; i += blockDim.x) fhist[i] = 0u;
   const int tw = diag_tile_w(n), th = diag_tile_h(n), per_row = tw / kDiagCells;
   const int tiles_x = n / tw;
@@ -395,10 +400,22 @@ __global__ void __launch_bounds__(256) k_diag_tiles(const float2* __restrict__ w
     atomicAdd(&fhist[nb + 1], fz);
   }
   __syncthreads();
-  // window bin r summed over the 32 lanes' windows (one warp per bin, lane = window)
-  for (int r = (int)(threadIdx.x >> 5); r < kDiagSpan; r += (int)(blockDim.x >> 5)) {
-    const double v = warp_sum(win[lane * kDiagStride + r]);
-    if (lane == 0 && v != 0.0 && lo + r < nb) atomicAdd(&out[lo + r], v);
+  // window bin r summed over the 32 lanes' windows in a fixed order: thread (g, r) adds
+  // lanes [11 g, 11 g + 11) of bin r and leaves the sum in the slot of lane 11 g (no other
+  // thread reads or writes bin r of those lanes), then thread r adds the three partials
+  static_assert(3 * kDiagSpan <= 256, "three partial sums per window bin");
+  if ((int)threadIdx.x < 3 * kDiagSpan) {
+    const int g = (int)threadIdx.x / kDiagSpan, r = (int)threadIdx.x - g * kDiagSpan;
+    const int l0 = 11 * g, l1 = min(l0 + 11, 32);
+    double v = win[l0 * kDiagStride + r];
+    for (int l = l0 + 1; l < l1; ++l) v += win[l * kDiagStride + r];
+    win[l0 * kDiagStride + r] = v;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < kDiagSpan) {
+    const int r = (int)threadIdx.x;
+    const double v = (win[r] + win[11 * kDiagStride + r]) + win[22 * kDiagStride + r];
+    if (v != 0.0 && lo + r < nb) atomicAdd(&out[lo + r], v);
   }
   if (threadIdx.x == 0) {
     atomicAdd(&out[nb], tot[0]);
