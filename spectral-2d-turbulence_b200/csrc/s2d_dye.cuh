@@ -384,15 +384,59 @@ __device__ __forceinline__ Rgb bilerp_rgb(const TF& tf, const Footprint& f, Rgb*
 // Window lookups without a bounds test, for a tile whose every trace moves less than one
 // texel: each footprint then lies inside its window by construction of the halos, and the
 // lookup reads the same slots (and does the same arithmetic) as the tested one above.
+// Footprint of a sample for window lookups: the unwrapped texel of its lower corner and
+// the weights (the arithmetic of footprint(); a window wraps the corner once, since
+// ((x & (m-1)) - o) & (m-1) is (x - o) & (m-1) for a power-of-two m)
+struct WinFoot {
+  int ix, iy;
+  float fx, fy;
+};
+__device__ __forceinline__ WinFoot win_foot(float sx, float sy, int m) {
+  const float mf = (float)m;
+  const float gx = __fmaf_rn(sx, mf, -0.5f), gy = __fmaf_rn(sy, mf, -0.5f);   // sx * mf exact
+  const float bx = floorf(gx), by = floorf(gy);
+  return {(int)bx, (int)by, __fsub_rn(gx, bx), __fsub_rn(gy, by)};
+}
 struct FastTex {   // binary16 window of row length W at wrapped origin (ox, oy)
   const uint2* sm;
   int w, ox, oy, m;
-  __device__ __forceinline__ Rgb sample(const Footprint& f, Rgb* lo = nullptr, Rgb* hi = nullptr) const {
-    const uint2* p = sm + ((f.y0 - oy) & (m - 1)) * w + ((f.x0 - ox) & (m - 1));
+  __device__ __forceinline__ const uint2* at(const WinFoot& f) const {
+    return sm + ((f.iy - oy) & (m - 1)) * w + ((f.ix - ox) & (m - 1));
+  }
+  __device__ __forceinline__ Rgb sample(const WinFoot& f, Rgb* lo = nullptr, Rgb* hi = nullptr) const {
+    const uint2* p = at(f);
     const Rgb q[4] = {rgb_of(p[0]), rgb_of(p[1]), rgb_of(p[w]), rgb_of(p[w + 1])};
-    return bilerp_quad(q, f, lo, hi);
+    Footprint fp;
+    fp.fx = f.fx;
+    fp.fy = f.fy;
+    return bilerp_quad(q, fp, lo, hi);
   }
 };
+// the corrected pass's two samples over one footprint: a from the source window (with
+// the 4-texel min / max), b from the backward window; r, g of each on the packed pipe as
+// in bilerp_quad, and the two b channels together in one packed chain (each lane the
+// arithmetic of lerp2)
+__device__ __forceinline__ void sample_corr(const FastTex& ta, const FastTex& tb, const WinFoot& f, Rgb& a, Rgb& b,
+                                            Rgb& lo, Rgb& hi) {
+  const uint2* pa = ta.at(f);
+  const uint2* pb = tb.at(f);
+  const Rgb a00 = rgb_of(pa[0]), a10 = rgb_of(pa[1]), a01 = rgb_of(pa[ta.w]), a11 = rgb_of(pa[ta.w + 1]);
+  const Rgb b00 = rgb_of(pb[0]), b10 = rgb_of(pb[1]), b01 = rgb_of(pb[tb.w]), b11 = rgb_of(pb[tb.w + 1]);
+  lo.r = fminf(fminf(a00.r, a10.r), fminf(a01.r, a11.r));
+  lo.g = fminf(fminf(a00.g, a10.g), fminf(a01.g, a11.g));
+  lo.b = fminf(fminf(a00.b, a10.b), fminf(a01.b, a11.b));
+  hi.r = fmaxf(fmaxf(a00.r, a10.r), fmaxf(a01.r, a11.r));
+  hi.g = fmaxf(fmaxf(a00.g, a10.g), fmaxf(a01.g, a11.g));
+  hi.b = fmaxf(fmaxf(a00.b, a10.b), fmaxf(a01.b, a11.b));
+  const float2 arg = lerp2v(lerp2v(make_float2(a00.r, a00.g), make_float2(a10.r, a10.g), f.fx),
+                            lerp2v(make_float2(a01.r, a01.g), make_float2(a11.r, a11.g), f.fx), f.fy);
+  const float2 brg = lerp2v(lerp2v(make_float2(b00.r, b00.g), make_float2(b10.r, b10.g), f.fx),
+                            lerp2v(make_float2(b01.r, b01.g), make_float2(b11.r, b11.g), f.fx), f.fy);
+  const float2 bb = lerp2v(lerp2v(make_float2(a00.b, b00.b), make_float2(a10.b, b10.b), f.fx),
+                           lerp2v(make_float2(a01.b, b01.b), make_float2(a11.b, b11.b), f.fx), f.fy);
+  a = {arg.x, arg.y, bb.x};
+  b = {brg.x, brg.y, bb.y};
+}
 struct FastVel {   // FP32 velocity window
   const float2* sm;
   int w, ox, oy, n;
@@ -537,10 +581,9 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
     const float2 sp = trace(p.x, p.y, v1, h);
     const int ix = rx - 2 * kDyeLo, iy = ry - 2 * kDyeLo;
     if ((unsigned)ix < (unsigned)TX && (unsigned)iy < (unsigned)TY) c.s_sp[iy * TX + ix] = sp;
-    const Footprint f = footprint(sp.x, sp.y, m);
     Rgb r;
-    if constexpr (FAST) r = FT.sample(f);
-    else r = bilerp_rgb(T, f);
+    if constexpr (FAST) r = FT.sample(win_foot(sp.x, sp.y, m));
+    else r = bilerp_rgb(T, footprint(sp.x, sp.y, m));
     c.s_fwd[i] = pack_rgb(r);
   }
   __syncthreads();
@@ -556,10 +599,9 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
     const int fi = (ry + kDyeLo) * W2X + rx + kDyeLo;
     const float2 p = texel_pos((c.bx0 + rx) & (m - 1), (c.by0 + ry) & (m - 1), inv_m);
     const float2 sb = trace(p.x, p.y, c.s_v1[fi], -h);
-    const Footprint f = footprint(sb.x, sb.y, m);
     Rgb r;
-    if constexpr (FAST) r = FFT.sample(f);
-    else r = bilerp_rgb(ff, f);
+    if constexpr (FAST) r = FFT.sample(win_foot(sb.x, sb.y, m));
+    else r = bilerp_rgb(ff, footprint(sb.x, sb.y, m));
     c.s_back[i] = pack_rgb(r);
   }
   __syncthreads();
@@ -572,12 +614,11 @@ __device__ __forceinline__ void dye_cta_passes(const DyeCta<TX>& c) {
     const int ry = i / TX, rx = i - ry * TX;
     const int x = c.tx0 + rx, y = c.ty0 + ry;
     const float2 sp = c.s_sp[i];
-    const Footprint f = footprint(sp.x, sp.y, m);
     Rgb lo, hi, a, b;
     if constexpr (FAST) {
-      a = FT.sample(f, &lo, &hi);
-      b = FB.sample(f);
+      sample_corr(FT, FB, win_foot(sp.x, sp.y, m), a, b, lo, hi);
     } else {
+      const Footprint f = footprint(sp.x, sp.y, m);
       a = bilerp_rgb(T, f, &lo, &hi);
       b = bilerp_rgb(bf, f);
     }
