@@ -353,11 +353,18 @@ static int flush_uploads(s2d_solver* s) {
     if (!(s)) return fail(S2D_ERR_ARG, "null solver handle");              \
     if ((s)->disposed) return fail(S2D_ERR_DESTROYED, "solver destroyed"); \
   } while (0)
+static bool stream_capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
 // the main stream waits for the outstanding spectra launch (see s2d_solver::diag_stream)
 static int diag_order(s2d_solver* s) {
   if (!s->diag_outstanding) return S2D_OK;
   s->diag_outstanding = false;
-  const cudaError_t e = cudaStreamWaitEvent(s->stream, s->diag_done, 0);
+  // a caller capturing the main stream into a graph: the graph runs later, after the
+  // spectra have finished on the host's clock
+  const cudaError_t e = stream_capturing(s->stream) ? cudaEventSynchronize(s->diag_done)
+                                                    : cudaStreamWaitEvent(s->stream, s->diag_done, 0);
   return e == cudaSuccess ? S2D_OK : fail(S2D_ERR_CUDA, std::string("diagnostics order: ") + cudaGetErrorString(e));
 }
 // Every entry point that enqueues device work (or reads the device) flushes the host
@@ -1256,15 +1263,25 @@ extern "C" int s2d_encode_diagnostics(s2d_solver* s) {
   // the zonal mean reads the velocity, which the next step rewrites: on the main stream
   k_diag_zonal<<<diag_zonal_ctas(n), 256, 0, s->stream>>>(s->vel, diag_zonal(s, b), n);
   S2D_LAUNCHED();
-  // the spectra of state[phase] on the diagnostics stream, alongside the next step
-  S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
-  S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
-  k_diag_tiles<<<diag_tiles(n), 256, diag_all_smem(n), s->diag_stream>>>(
+  // the spectra of state[phase] on the diagnostics stream, alongside the next step (on the
+  // main stream while a caller captures it into a graph of its own)
+  const bool side = !stream_capturing(s->stream);
+  if (side) {
+    S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
+    S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
+  } else {
+    // a captured graph may run any number of times: it clears the block it fills itself
+    S2D_CUDA(cudaMemsetAsync(diag_fp64(s, b), 0, (sizeof(double) + sizeof(uint32_t)) * (size_t)(s->nbins + 2),
+                             s->stream));
+  }
+  k_diag_tiles<<<diag_tiles(n), 256, diag_all_smem(n), side ? s->diag_stream : s->stream>>>(
       s->state[s->phase], diag_fp64(s, b), diag_u32(s, b), n, diag_fp64(s, 1 - b), diag_u32(s, 1 - b));
   S2D_LAUNCHED();
-  S2D_CUDA(cudaEventRecord(s->diag_done, s->diag_stream));
-  s->diag_outstanding = true;
-  s->diag_age = 0;
+  if (side) {
+    S2D_CUDA(cudaEventRecord(s->diag_done, s->diag_stream));
+    s->diag_outstanding = true;
+    s->diag_age = 0;
+  }
   s->diag_last = b;
   s->diag_next = 1 - b;
   return S2D_OK;
@@ -1274,18 +1291,22 @@ extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
   S2D_USE_NOORDER(s);
   if (s->read_state != 0) return S2D_OK;    // solver.js:561-563
   DeviceGuard guard(s->dev);
-  // on the diagnostics stream, behind the spectra and the main stream's work so far: the
-  // block last filled, and the [dt, speed] slot current now
-  S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
-  S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
+  // on the diagnostics stream, behind the spectra and the main stream's work so far (on the
+  // main stream while a caller captures it): the block last filled, and the [dt, speed]
+  // slot current now
+  const bool side = !stream_capturing(s->stream);
+  if (side) {
+    S2D_CUDA(cudaEventRecord(s->diag_ready, s->stream));
+    S2D_CUDA(cudaStreamWaitEvent(s->diag_stream, s->diag_ready, 0));
+  }
+  const cudaStream_t st = side ? s->diag_stream : s->stream;
   const int b = s->diag_last;
   const size_t off = diag_block_offset(s->nbins, s->n, b);
   S2D_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(s->h_base) + off, reinterpret_cast<char*>(s->diag) + off,
-                           diag_block_bytes(s->nbins, s->n), cudaMemcpyDeviceToHost, s->diag_stream));
-  S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), 2 * sizeof(float), cudaMemcpyDeviceToHost,
-                           s->diag_stream));
+                           diag_block_bytes(s->nbins, s->n), cudaMemcpyDeviceToHost, st));
+  S2D_CUDA(cudaMemcpyAsync(s->h_dt, dt_slot(s, s->slot), 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
   set_host_diag_block(s, b);
-  S2D_CUDA(cudaEventRecord(s->diag_event, s->diag_stream));
+  S2D_CUDA(cudaEventRecord(s->diag_event, st));
   s->read_state = 1;
   return S2D_OK;
 }

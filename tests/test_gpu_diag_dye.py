@@ -81,6 +81,34 @@ def test_diagnostics_run_alongside_the_next_steps(pkg, graph):
     _same_diagnostics(d2, once, "second encode")
 
 
+def test_diagnostics_captured_by_the_caller(pkg):
+    """encodeDiagnostics captured into a caller's graph on the solver's stream (the spectra
+    then stay on that stream, and the graph clears the block it fills): replayed three
+    times, it gives the diagnostics of the state, as a plain call does."""
+    import torch
+    n = 128
+    s = pkg.Solver.create(n=n, dyeScale=2)
+    try:
+        s.configure(config(viscosity=1.0, cfl=0.5, dtMax=0.01))
+        s.seedPhysical(random_field(n, k0=12, seed=6, amplitude=5.0))
+        s.step(2, dye=True, reduce=True, graph=True)
+        s.encodeDiagnostics(); s.copyDiagnostics()
+        ref = s.readDiagnostics()
+        s.synchronize()
+        st = torch.cuda.ExternalStream(s.stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            s.encodeDiagnostics()
+        for _ in range(3):
+            g.replay()
+        st.synchronize()
+        s.copyDiagnostics()
+        _same_diagnostics(s.readDiagnostics(), ref, "captured")
+        del g
+    finally:
+        s.destroy()
+
+
 def test_pipelined_readback_matches_synchronous(pkg):
     """The frame-loop order of the end-to-end benchmark (step k, encode k, read k-1,
     copy k) gives, for every step, the diagnostics a synchronous encode-copy-read of the
