@@ -14,8 +14,11 @@
  * ky = wn(row), column = x index with kx = wn(col), wn(i) = i < N/2 ? i : i-N.
  * The dye is M*M texels of 4 binary16 values (rgba16float), M = N*dye_scale.
  *
- * Threading: a solver handle is used from one host thread at a time; all GPU
- * work of one solver is ordered on the solver's own CUDA stream.
+ * Threading: a solver handle is used from one host thread at a time (except
+ * s2d_poll_diagnostics, host-only, which another thread may call); the GPU work of
+ * one solver runs on the solver's own CUDA stream, except the diagnostics spectra
+ * and readback copies, which run on a second stream of the solver and are ordered
+ * against the first by the library (s2d_encode_diagnostics).
  */
 #ifndef S2D_H
 #define S2D_H
@@ -159,8 +162,8 @@ int s2d_probe_wait_timeout(s2d_solver* s, unsigned long long limit_ns);
 /* Both update the solver's host copy of the parameter / splat block and return; the
  * blocks that changed reach the device together, in one copy from pinned memory, at the
  * start of the next call that enqueues device work or reads the device (every s2d_*
- * call on the solver except these two, s2d_get_info, s2d_set_phase, s2d_set_sim_time and
- * s2d_get_stream) -- in stream order before that call's work, as the reference's
+ * call on the solver except these two, s2d_get_info, s2d_set_phase, s2d_set_sim_time,
+ * s2d_get_stream and s2d_poll_diagnostics) -- in stream order before that call's work, as the reference's
  * writeBuffer precedes the passes encoded after it.  Work a caller enqueues on the
  * solver's stream directly sees the blocks after the next such call. */
 int s2d_configure(s2d_solver* s, const s2d_params* p);                   /* solver.js:306-324 */

@@ -759,7 +759,12 @@ extern "C" int s2d_get_info(s2d_solver* s, s2d_info* out) {
 extern "C" int s2d_set_phase(s2d_solver* s, int phase, int dye_parity) {
   S2D_USE_HOST(s);
   if (phase < 0 || phase > 2 || dye_parity < 0 || dye_parity > 1) return fail(S2D_ERR_ARG, "phase out of range");
-  if (phase != s->phase) s->packs_valid = false;
+  if (phase != s->phase) {
+    // the next step writes other ring buffers: none may be one the outstanding spectra read
+    DeviceGuard guard(s->dev);
+    if (int rc = diag_order(s)) return rc;
+    s->packs_valid = false;
+  }
   s->phase = phase;
   s->dye_parity = dye_parity;
   return S2D_OK;
@@ -1311,8 +1316,9 @@ extern "C" int s2d_copy_diagnostics(s2d_solver* s) {
   return S2D_OK;
 }
 
+// host-only (no upload flush): the Node-API addon polls from a worker thread
 extern "C" int s2d_poll_diagnostics(s2d_solver* s) {
-  S2D_USE_NOORDER(s);
+  S2D_USE_HOST(s);
   if (s->read_state != 1) return 0;
   return cudaEventQuery(s->diag_event) == cudaSuccess ? 1 : 0;
 }

@@ -65,6 +65,9 @@ def test_diagnostics_run_alongside_the_next_steps(pkg, graph):
         "three steps": lambda s: [s.step(1, dye=True, reduce=True, graph=graph) for _ in range(3)],
         "substeps": lambda s: s.step(4, dye=True, reduce=True, graph=graph),
         "reseed": lambda s: s.seed(k0=9, amplitude=3, seed=5),
+        # a phase moved back one place makes the next step write the buffer just read
+        "phase moved": lambda s: (setattr(s, "phase", (s.phase + 2) % 3),
+                                  s.step(1, dye=True, reduce=True, graph=graph)),
     }
     for name, between in cases.items():
         d, dt_now = _diag_after_steps(pkg, n, 3, graph, between)
