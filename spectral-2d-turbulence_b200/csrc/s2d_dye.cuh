@@ -89,8 +89,14 @@ __device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - 
 // (0.5 (v h) is v (h/2): halving commutes with the rounding of the product)
 // fract(p - v s + 1) on both coordinates with the packed pipe (same bits as fract_shift:
 // p - d is p + (-d), and the negation is exact)
+// The product v s is rounded before the sum, as in the scalar form: it is formed as a
+// fused multiply-add with a +0 addend, which no compiler may turn back into a multiply (it
+// differs from one in the sign of a zero product) and so into a multiply-add with p.  A
+// packed multiply followed by a packed add -- __fmul2_rn / __fadd2_rn, and PTX mul.rn /
+// add.rn on f32x2 alike -- was measured contracted into one FFMA2 (one FP32 unit apart in
+// ~1e-4 of the trace positions).  p is a texel centre, never zero, so p + (+0) is p.
 __device__ __forceinline__ float2 fract_shift2(float2 p, float2 v, float s) {
-  const float2 d = __fmul2_rn(v, make_float2(-s, -s));
+  const float2 d = __ffma2_rn(v, make_float2(-s, -s), make_float2(0.f, 0.f));
   const float2 x = __fadd2_rn(__fadd2_rn(p, d), make_float2(1.f, 1.f));
   return make_float2(__fsub_rn(x.x, floorf(x.x)), __fsub_rn(x.y, floorf(x.y)));
 }

@@ -260,12 +260,9 @@ def test_dye_bfecc_step(pkg, m_scale):
         want_bits = wo.dye_step(dye0, velf, dt, 0.999, [_splat_np(splat)])
         want = wo.half_bits_to_f32(want_bits)
         # the restatement evaluates the kernels' FP32 operations in the same order with the
-        # same fused multiply-adds.  Texels untouched by the splat: every binary16 channel
-        # within one unit in the last place and at most 1e-4 of them off by that unit (this
-        # case measured 0 of 49152 channels at dyeScale 1 and 3 of 196608 at dyeScale 2,
-        # each explained by one forward- or backward-pass texel one unit apart upstream).
-        # Inside the splat the weight uses expf, whose CUDA and NumPy results may differ in
-        # the last FP32 bit: one unit in the last place, on at most 1 % of the channels.
+        # same fused multiply-adds: texels untouched by the splat are bit-exact.  Inside the
+        # splat the weight uses expf, whose CUDA and NumPy results may differ in the last
+        # FP32 bit: one unit in the last place, on at most 1 % of the channels.
         px = (np.arange(n * m_scale) + 0.5) / (n * m_scale)
         rx = (px[None, :] - splat["x"] + 0.5) % 1.0 - 0.5
         ry = (px[:, None] - splat["y"] + 0.5) % 1.0 - 0.5
@@ -273,8 +270,7 @@ def test_dye_bfecc_step(pkg, m_scale):
         gb = s.currentDye.astype(np.int32)
         wb = want_bits.astype(np.int32)
         far = ~near
-        assert np.max(np.abs(gb[far] - wb[far])) <= 1
-        assert np.mean(gb[far] != wb[far]) <= 1e-4, int(np.count_nonzero(gb[far] != wb[far]))
+        assert np.array_equal(gb[far], wb[far]), int(np.count_nonzero(gb[far] != wb[far]))
         assert np.max(np.abs(gb[near] - wb[near])) <= 1
         assert np.mean(gb[near] != wb[near]) <= 1e-2
         assert np.all(got[..., 3] == 1.0)
