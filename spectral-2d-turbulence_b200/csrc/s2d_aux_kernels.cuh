@@ -366,7 +366,9 @@ __global__ void __launch_bounds__(256) k_diag_tiles(const float2* __restrict__ w
       }
       // u32 fixed point
       if (k2f != 0.f && fabsf(kxf) < kcut && fabsf(kyf) < kcut) {
-        const float ensf = 0.5f * (a.x * a.x + a.y * a.y) * inv_n4f;
+        // both squares rounded before the sum (no multiply-add contraction), as the
+        // reference's f32 expression is written; the scalings are exact
+        const float ensf = 0.5f * __fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)) * inv_n4f;
         const float enef = ensf / k2f;
         const int fb = (int)min((uint32_t)fb_raw, (uint32_t)(nb - 1));
         if (fb != cur_fb) {
