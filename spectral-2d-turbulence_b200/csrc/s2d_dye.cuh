@@ -80,21 +80,16 @@ __device__ __forceinline__ float2 sample_vel(const VF& vf, float px, float py, i
   return lerp2v(lerp2v(v00, v10, fx), lerp2v(v01, v11, fx), fy);
 }
 
-__device__ __forceinline__ float fract_shift(float p, float d) {   // fract(p - d + 1)
-  const float x = __fadd_rn(__fsub_rn(p, d), 1.f);
-  return __fsub_rn(x, floorf(x));
-}
-
 // midpoint back-trace (dye.wgsl:40-45), from the velocity v1 already sampled at p
 // (0.5 (v h) is v (h/2): halving commutes with the rounding of the product)
-// fract(p - v s + 1) on both coordinates with the packed pipe (same bits as fract_shift:
-// p - d is p + (-d), and the negation is exact)
-// The product v s is rounded before the sum, as in the scalar form: it is formed as a
-// fused multiply-add with a +0 addend, which no compiler may turn back into a multiply (it
-// differs from one in the sign of a zero product) and so into a multiply-add with p.  A
-// packed multiply followed by a packed add -- __fmul2_rn / __fadd2_rn, and PTX mul.rn /
-// add.rn on f32x2 alike -- was measured contracted into one FFMA2 (one FP32 unit apart in
-// ~1e-4 of the trace positions).  p is a texel centre, never zero, so p + (+0) is p.
+// fract(p - v s + 1) on both coordinates with the packed pipe, as fract(p - d + 1) with
+// d = v s rounded: p - d is p + (-d), and the negation is exact.  The product is rounded
+// before the sum: it is formed as a fused multiply-add with a +0 addend, which no compiler
+// may turn back into a multiply (it differs from one in the sign of a zero product) and so
+// into a multiply-add with p.  A packed multiply followed by a packed add -- __fmul2_rn /
+// __fadd2_rn, and PTX mul.rn / add.rn on f32x2 alike -- was measured contracted into one
+// FFMA2 (one FP32 unit apart in ~1e-4 of the trace positions).  p is a texel centre, never
+// zero, so p + (+0) is p.
 __device__ __forceinline__ float2 fract_shift2(float2 p, float2 v, float s) {
   const float2 d = __ffma2_rn(v, make_float2(-s, -s), make_float2(0.f, 0.f));
   const float2 x = __fadd2_rn(__fadd2_rn(p, d), make_float2(1.f, 1.f));
