@@ -102,9 +102,10 @@ def test_diagnostics_captured_by_the_caller(pkg):
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=st):
             s.encodeDiagnostics()
-        for _ in range(3):
-            g.replay()
-        st.synchronize()
+        with torch.cuda.stream(st):   # replayed on the solver's stream, in its order
+            for _ in range(3):
+                g.replay()
+        torch.cuda.synchronize()
         s.copyDiagnostics()
         _same_diagnostics(s.readDiagnostics(), ref, "captured")
         del g
