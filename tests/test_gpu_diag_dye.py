@@ -242,7 +242,7 @@ def _splat_np(sp):
     return r
 
 
-@pytest.mark.parametrize("m_scale", [1, 2])
+@pytest.mark.parametrize("m_scale", [1, 2, 4])
 def test_dye_bfecc_step(pkg, m_scale):
     n = 128
     s = pkg.Solver.create(n=n, dyeScale=m_scale)
